@@ -1,0 +1,385 @@
+/*
+ * phraya_gpu.h -- C ABI of the B200 (sm_100a) seed -> chain -> extend engine.
+ *
+ * Every entry point is a plain C function over caller-owned buffers: pointers, sizes
+ * and POD structs only. Host-buffer entry points copy inputs to HBM, run the CUDA
+ * kernels and copy results back; "_device" entry points take device pointers and keep
+ * results resident. There is no CPU fallback: if the CUDA library cannot run, every
+ * compute call returns PHR_ERR_CUDA.
+ *
+ * Conventions shared with phraya-align (the Rust crate this replaces):
+ *   - CIGAR text uses the reference's letters: M (match), X (mismatch),
+ *     D = query-extra base, I = target-extra base  (phraya-align/src/wfa_simd.rs:1101-1105).
+ *   - Status codes map 1:1 onto WfaError (phraya-align/src/lib.rs:44-49):
+ *     PHR_INVALID_INPUT == WfaError::InvalidInput, PHR_ALIGNMENT_FAILED ==
+ *     WfaError::AlignmentFailed; the rest are engine errors with no Rust counterpart.
+ *   - A phr_ctx is bound to one device and one stream; it is not thread-safe. Use one
+ *     context per host thread (or wrap it in a mutex).
+ */
+#ifndef PHRAYA_GPU_H
+#define PHRAYA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHR_ABI_VERSION 1
+
+typedef enum {
+    PHR_OK = 0,
+    PHR_INVALID_INPUT = 1,     /* WfaError::InvalidInput (seed beyond sequence end)   */
+    PHR_ALIGNMENT_FAILED = 2,  /* WfaError::AlignmentFailed (search exhausted)         */
+    PHR_ERR_OOM = 3,           /* device allocation failed / not enough free HBM      */
+    PHR_ERR_TIMEOUT = 4,       /* a bounded device wait gave up                        */
+    PHR_ERR_CUDA = 5,          /* CUDA runtime error or no usable device               */
+    PHR_ERR_ARG = 6,           /* bad argument: NULL pointer, size over a stated limit */
+    PHR_ERR_CAPACITY = 7,      /* caller-supplied output arena too small               */
+    PHR_ERR_STATE = 8          /* call out of order (e.g. server not started)          */
+} phr_status;
+
+/* Extension engines, one per phraya-align entry point. */
+typedef enum {
+    PHR_ENGINE_WFA_LINEAR = 0,   /* wfa_extend            phraya-align/src/lib.rs:74      */
+    PHR_ENGINE_WFA_AFFINE = 1,   /* wfa_extend_affine     phraya-align/src/lib.rs:139-167 */
+    PHR_ENGINE_MYERS_FIT = 2,    /* myers_extend          phraya-align/src/lib.rs:106-127 */
+    PHR_ENGINE_MYERS_GLOBAL = 3  /* myers_edit_distance   phraya-align/src/lib.rs:94-96   */
+} phr_engine;
+
+/* AffineCosts (phraya-align/src/wfa_simd.rs:521-540); default {2,4,1}. */
+typedef struct {
+    int32_t mismatch;
+    int32_t gap_open;
+    int32_t gap_extend;
+} phr_affine_costs;
+
+/*
+ * A batch of query/target pairs (structure of arrays over one byte arena).
+ * Pair i aligns seq[q_off[i] .. q_off[i]+q_len[i]) [q_seed[i]..] against
+ * seq[t_off[i] .. t_off[i]+t_len[i]) [t_seed[i]..]  -- the SeedAnchor of lib.rs:25-28.
+ * q_seed / t_seed may be NULL (anchor (0,0)). Bytes are compared exactly as given
+ * (case-sensitive, N == N), as the reference does.
+ */
+typedef struct {
+    uint64_t n_pairs;
+    const uint8_t* seq;
+    uint64_t seq_bytes;
+    const uint64_t* q_off;
+    const uint32_t* q_len;
+    const uint64_t* t_off;
+    const uint32_t* t_len;
+    const uint32_t* q_seed;
+    const uint32_t* t_seed;
+} phr_pair_batch;
+
+/*
+ * One Alignment (phraya-align/src/lib.rs:31-39). The CIGAR is
+ * arena.cigar[cigar_off .. cigar_off + cigar_len), not NUL-terminated.
+ * For PHR_ENGINE_MYERS_GLOBAL the coordinates are (0, |q|, 0, |t|).
+ */
+typedef struct {
+    int32_t status;          /* phr_status of this pair (PHR_OK, PHR_INVALID_INPUT, ...) */
+    uint32_t edit_distance;
+    uint32_t query_start;
+    uint32_t query_end;
+    uint32_t target_start;
+    uint32_t target_end;
+    uint64_t cigar_off;
+    uint32_t cigar_len;
+    uint32_t affine_score;   /* WFA affine search score (0 for other engines) */
+} phr_alignment;
+
+/* Caller-owned result arena. cigar_used is written by the call. */
+typedef struct {
+    phr_alignment* aln;      /* n_pairs entries */
+    char* cigar;
+    uint64_t cigar_capacity;
+    uint64_t cigar_used;
+} phr_result_arena;
+
+/* Upper bound of the CIGAR bytes one pair can produce: 2 * (|q| + |t|). */
+#define PHR_CIGAR_BOUND(qlen, tlen) (2ull * ((uint64_t)(qlen) + (uint64_t)(tlen)))
+
+/* ------------------------------------------------------------------------- */
+/* Context                                                                    */
+/* ------------------------------------------------------------------------- */
+
+typedef struct phr_ctx phr_ctx;
+
+typedef struct {
+    uint64_t workspace_bytes;  /* device scratch reserved up front; 0 = default (1 GiB) */
+    int32_t tune_file_enable;  /* 1 = read/write autotuner cache file                   */
+    const char* tune_file;     /* NULL = "phraya_b200_tune.txt" in the working dir      */
+} phr_config;
+
+/* Reports the ABI version compiled into the library. */
+int32_t phr_abi_version(void);
+const char* phr_status_string(phr_status s);
+
+phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out);
+void phr_ctx_destroy(phr_ctx* ctx);
+/* Message describing the last non-PHR_OK status returned on this context. */
+const char* phr_ctx_last_error(const phr_ctx* ctx);
+/* Number of the library's own kernel launches issued on this context so far. */
+uint64_t phr_ctx_kernel_launches(const phr_ctx* ctx);
+
+/* ------------------------------------------------------------------------- */
+/* Pairs API -- replaces per-call wfa_extend / wfa_extend_affine /            */
+/* myers_extend / myers_edit_distance (phraya-align/src/lib.rs:63-167).       */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * Aligns every pair of `batch` (host memory) with `engine` and writes one
+ * phr_alignment per pair plus packed CIGAR text into `out` (host memory).
+ * `costs` is read only by PHR_ENGINE_WFA_AFFINE. Pairs are independent; per-pair
+ * failures are reported in phr_alignment.status, the call itself returns PHR_OK.
+ */
+phr_status phr_extend_batch(phr_ctx* ctx, phr_engine engine, const phr_pair_batch* batch,
+                            phr_affine_costs costs, phr_result_arena* out);
+
+/*
+ * Same as phr_extend_batch, but every pointer in `batch` and `out` is DEVICE memory
+ * (out->aln, out->cigar). Work is queued on the context's stream; the call returns
+ * after the results are complete in device memory. Used by callers that keep data
+ * resident in HBM.
+ */
+phr_status phr_extend_batch_device(phr_ctx* ctx, phr_engine engine, const phr_pair_batch* batch,
+                                   phr_affine_costs costs, phr_result_arena* out);
+
+/*
+ * Per-call variant: one launch sequence per pair, the shape of the reference's
+ * one-call-per-pair API. Exists as the baseline the batched path is measured against.
+ */
+phr_status phr_extend_percall(phr_ctx* ctx, phr_engine engine, const phr_pair_batch* batch,
+                              phr_affine_costs costs, phr_result_arena* out);
+
+/* ------------------------------------------------------------------------- */
+/* Sketches, target index, seeding and chaining                               */
+/* ------------------------------------------------------------------------- */
+
+typedef enum { PHR_ALPHABET_DNA = 0, PHR_ALPHABET_PROTEIN = 1 } phr_alphabet;
+
+/* MinimizerSketch (phraya-core/src/types.rs:1803-1810) as two parallel arrays. */
+typedef struct {
+    const uint64_t* values;
+    const uint32_t* positions;
+    uint64_t n;
+    int32_t k;
+    int32_t w;
+} phr_sketch;
+
+typedef struct phr_index phr_index;
+
+typedef struct {
+    uint64_t n_minimizers;     /* target sketch length                          */
+    uint64_t n_distinct;       /* distinct minimizer values                     */
+    uint64_t occurrence_cap;   /* seed_occurrence_cap(index, 256)               */
+    uint64_t target_len;
+    uint64_t device_bytes;     /* HBM held by the index                         */
+} phr_index_info;
+
+/*
+ * TargetContext::build (phraya-align/src/executor.rs:431-449): uploads the target
+ * bytes, builds the minimizer index (build_minimizer_index, seeding.rs:31-37) and the
+ * occurrence cap (seed_occurrence_cap(index, 256), seeding.rs:94-102) on the device.
+ * `sketch` may be NULL: the target is then sketched with the library's sketcher at the
+ * alphabet's default k/w (DNA 21/11 canonical, protein 6/5 plain).
+ */
+phr_status phr_index_create(phr_ctx* ctx, const uint8_t* target, uint64_t target_len,
+                            const phr_sketch* sketch, phr_alphabet alphabet, phr_index** out);
+void phr_index_destroy(phr_index* idx);
+phr_status phr_index_get_info(const phr_index* idx, phr_index_info* info);
+
+/*
+ * The library's minimizer sketcher: canonical (DNA) or plain (protein) (k, w)
+ * minimizers of every sequence in the batch. Stands in for simd-minimizers at
+ * phraya-core/src/types.rs:1848-1869 (the same function the oracle restates).
+ * Sequence i is seq[off[i] .. off[i]+len[i]). Output: sequence i's minimizers at
+ * values/positions[out_off[i] .. out_off[i] + out_n[i]); capacity per sequence is
+ * max(len[i] - k + 1, 0) entries, so out_off must leave that much room.
+ */
+typedef struct {
+    uint64_t n;
+    const uint8_t* seq;
+    uint64_t seq_bytes;
+    const uint64_t* off;
+    const uint32_t* len;
+} phr_seq_batch;
+
+phr_status phr_sketch_batch(phr_ctx* ctx, const phr_seq_batch* seqs, int32_t k, int32_t w,
+                            phr_alphabet alphabet, const uint64_t* out_off, uint64_t* values,
+                            uint32_t* positions, uint32_t* out_n);
+
+/* Chain (phraya-align/src/chaining.rs:24-35): seeds and score. */
+typedef struct {
+    uint32_t query_pos;
+    uint32_t target_pos;
+    uint64_t minimizer;
+} phr_seed;
+
+typedef struct {
+    int64_t score;
+    uint32_t seed_off;         /* into phr_chain_arena.seeds */
+    uint32_t n_seeds;
+    uint32_t target_start;     /* Chain::target_start()      */
+    uint32_t _pad;
+} phr_chain;
+
+typedef struct {
+    /* per query: chains[chain_off[i] .. chain_off[i] + n_chains[i]) */
+    uint32_t* n_seeds_found;   /* raw seed count (find_seeds_indexed_capped length) */
+    uint32_t* n_chains;
+    uint64_t* chain_off;       /* written by the call */
+    phr_chain* chains;
+    uint64_t chain_capacity;
+    phr_seed* seeds;
+    uint64_t seed_capacity;
+} phr_chain_arena;
+
+/*
+ * seed_and_chain (phraya-align/src/executor.rs:511-519) for every query sketch:
+ * find_seeds_indexed_capped (seeding.rs:58-80) against the index with its occurrence
+ * cap, then chain_seeds with ChainParams::default() (chaining.rs:134-226).
+ * sketches[i] are host arrays.
+ */
+phr_status phr_seed_chain_batch(phr_ctx* ctx, const phr_index* idx, const phr_sketch* sketches,
+                                uint64_t n_queries, phr_chain_arena* out);
+
+/* ------------------------------------------------------------------------- */
+/* align_read -- the whole per-read pipeline up to `scored`                   */
+/* (phraya-align/src/executor.rs:573-733, 777-787)                            */
+/* ------------------------------------------------------------------------- */
+
+typedef enum { PHR_FAST = 0, PHR_BALANCED = 1, PHR_SENSITIVE = 2 } phr_strategy;
+typedef enum { PHR_GAP_LINEAR = 0, PHR_GAP_AFFINE = 1 } phr_gap_model;
+
+/* AlignConfig (executor.rs:107-166) minus the coverage radius, which only feeds
+ * host-side variant extraction. */
+typedef struct {
+    phr_strategy strategy;
+    phr_gap_model gap_model;   /* consulted only for PHR_SENSITIVE */
+} phr_align_config;
+
+/*
+ * Reads: seq[off[i] .. off[i]+len[i]). Optional stored forward sketches
+ * (plan.get_read_sketch, executor.rs:615-624): when has_stored[i] != 0, read i uses
+ * sketch values/positions[s_off[i] .. s_off[i]+s_n[i]) as its forward sketch
+ * (an empty stored sketch with no seeds means NoSeed, executor.rs:671-674).
+ * All four stored-sketch pointers may be NULL.
+ */
+typedef struct {
+    uint64_t n_reads;
+    const uint8_t* seq;
+    uint64_t seq_bytes;
+    const uint64_t* off;
+    const uint32_t* len;
+    const uint8_t* has_stored;
+    const uint64_t* s_off;
+    const uint32_t* s_n;
+    const uint64_t* s_values;
+    const uint32_t* s_positions;
+} phr_read_batch;
+
+/* AlignStats outcome buckets (executor.rs:269-322). */
+typedef enum {
+    PHR_OUT_PLACED = 0,
+    PHR_OUT_NO_SEED = 1,
+    PHR_OUT_BELOW_THRESHOLD = 2,
+    PHR_OUT_FAST_CUTOFF = 3,
+    PHR_OUT_NO_ALIGNMENT = 4
+} phr_outcome;
+
+/*
+ * Per read: the winning orientation's ScoredAlignments (primary first, then the
+ * alternatives with score ratio >= 0.95, lib.rs:170-199) as alignments
+ * aln[aln_off .. aln_off + n_aln); `reverse` = 1 when the reverse complement won.
+ * has_result = 0 when align_read would return None (NoAlignment, FastCutoff, stored
+ * empty sketch); `outcome` is always set. query_positions of the reference
+ * (executor.rs:777-781) are (aln.target_start, 1 - aln.edit_distance / max(|q|,1)).
+ */
+typedef struct {
+    int32_t outcome;
+    uint8_t has_result;
+    uint8_t reverse;
+    uint16_t _pad;
+    uint32_t n_aln;
+    uint32_t _pad2;
+    uint64_t aln_off;
+} phr_read_result;
+
+typedef struct {
+    phr_read_result* reads;    /* n_reads entries */
+    phr_alignment* aln;
+    uint64_t aln_capacity;
+    uint64_t aln_used;
+    char* cigar;
+    uint64_t cigar_capacity;
+    uint64_t cigar_used;
+} phr_read_result_arena;
+
+typedef struct {
+    uint64_t placed;
+    uint64_t no_seed;
+    uint64_t below_threshold;
+    uint64_t fast_cutoff;
+    uint64_t no_alignment;
+} phr_align_stats;
+
+/*
+ * align_read for every read of the batch against `idx`, bit-exact with
+ * phraya-align's executor. `stats` may be NULL; when given, outcomes are ADDED to it.
+ */
+phr_status phr_align_reads(phr_ctx* ctx, const phr_index* idx, const phr_read_batch* reads,
+                           const phr_align_config* cfg, phr_read_result_arena* out,
+                           phr_align_stats* stats);
+
+/* ------------------------------------------------------------------------- */
+/* Serving loop: device-resident index, admission by free HBM, continuous    */
+/* batching. No counterpart in the reference (its CLI is batch-only).         */
+/* ------------------------------------------------------------------------- */
+
+typedef struct phr_server phr_server;
+
+typedef struct {
+    phr_align_config align;
+    uint32_t max_batch_reads;      /* reads per device batch (0 = 4096)            */
+    uint64_t max_batch_bases;      /* bases per device batch (0 = 16 Mbp)          */
+    uint64_t hbm_reserve_bytes;    /* free HBM kept back when admitting (0 = 2 GiB) */
+    uint32_t max_wait_us;          /* batch-forming window after first arrival     */
+    uint32_t n_streams;            /* concurrent batches in flight (0 = 2)         */
+} phr_server_config;
+
+typedef struct {
+    uint64_t request_id;
+    int32_t outcome;
+    uint8_t has_result;
+    uint8_t reverse;
+    uint16_t _pad;
+    uint32_t n_aln;
+    uint32_t _pad2;
+    double latency_us;             /* submit -> result ready */
+} phr_server_result;
+
+phr_status phr_server_create(phr_ctx* ctx, const phr_index* idx, const phr_server_config* cfg,
+                             phr_server** out);
+/* Enqueues one read (bytes copied); returns its request id in *request_id. */
+phr_status phr_server_submit(phr_server* srv, const uint8_t* read, uint32_t len,
+                             uint64_t* request_id);
+/*
+ * Copies up to `max_results` finished requests into `res` (and their alignments and
+ * CIGARs, packed, into the given arrays), returns how many in *n_out.
+ * `wait_us` > 0 blocks up to that long for at least one result.
+ */
+phr_status phr_server_poll(phr_server* srv, phr_server_result* res, uint32_t max_results,
+                           phr_alignment* aln, uint64_t aln_capacity, char* cigar,
+                           uint64_t cigar_capacity, uint32_t wait_us, uint32_t* n_out);
+/* Stops after draining every submitted request. */
+phr_status phr_server_destroy(phr_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHRAYA_GPU_H */
