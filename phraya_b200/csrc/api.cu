@@ -1,0 +1,235 @@
+// api.cu -- C ABI entry points (include/phraya_gpu.h): context and pairs API.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "engine.cuh"
+
+using phr::Ctx;
+
+struct phr_ctx {
+    Ctx impl;
+};
+
+namespace {
+
+phr_status check_ctx(phr_ctx* c) { return c ? PHR_OK : PHR_ERR_ARG; }
+
+// Copies a host pair batch into the context's io arena and returns device views.
+phr_status upload_pairs(Ctx* ctx, const phr_pair_batch* b, phr::DevPairs* dp, uint64_t* sum_qt, size_t extra) {
+    const uint64_t n = b->n_pairs;
+    uint64_t s = 0;
+    for (uint64_t i = 0; i < n; ++i) s += static_cast<uint64_t>(b->q_len[i]) + b->t_len[i];
+    *sum_qt = s;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (b->q_off[i] + b->q_len[i] > b->seq_bytes || b->t_off[i] + b->t_len[i] > b->seq_bytes)
+            return phr::set_error(ctx, PHR_ERR_ARG, "pair " + std::to_string(i) + " reaches past seq_bytes");
+    }
+    const size_t need = b->seq_bytes + 64 + n * (8 + 4 + 8 + 4 + 4 + 4) + 8 * 256 + extra;
+    ctx->io.reset();
+    PHR_CUDA_TRY(ctx, ctx->io.reserve(need));
+    auto take = [&](size_t bytes) { return ctx->io.take(bytes); };
+    uint8_t* seq = static_cast<uint8_t*>(take(b->seq_bytes + 64));
+    uint64_t* qo = static_cast<uint64_t*>(take(n * 8));
+    uint32_t* ql = static_cast<uint32_t*>(take(n * 4));
+    uint64_t* to = static_cast<uint64_t*>(take(n * 8));
+    uint32_t* tl = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* qs = b->q_seed ? static_cast<uint32_t*>(take(n * 4)) : nullptr;
+    uint32_t* ts = b->t_seed ? static_cast<uint32_t*>(take(n * 4)) : nullptr;
+    cudaStream_t st = ctx->stream;
+    if (b->seq_bytes) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(seq, b->seq, b->seq_bytes, cudaMemcpyHostToDevice, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(qo, b->q_off, n * 8, cudaMemcpyHostToDevice, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(ql, b->q_len, n * 4, cudaMemcpyHostToDevice, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(to, b->t_off, n * 8, cudaMemcpyHostToDevice, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(tl, b->t_len, n * 4, cudaMemcpyHostToDevice, st));
+    if (qs) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(qs, b->q_seed, n * 4, cudaMemcpyHostToDevice, st));
+    if (ts) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(ts, b->t_seed, n * 4, cudaMemcpyHostToDevice, st));
+    dp->n = n;
+    dp->seq = seq;
+    dp->seq_bytes = b->seq_bytes;
+    dp->q_off = qo;
+    dp->q_len = ql;
+    dp->t_off = to;
+    dp->t_len = tl;
+    dp->q_seed = qs;
+    dp->t_seed = ts;
+    return PHR_OK;
+}
+
+bool valid_engine(phr_engine e) {
+    return e == PHR_ENGINE_WFA_LINEAR || e == PHR_ENGINE_WFA_AFFINE || e == PHR_ENGINE_MYERS_FIT ||
+           e == PHR_ENGINE_MYERS_GLOBAL;
+}
+
+phr_status extend_host(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                       phr_result_arena* out) {
+    Ctx* ctx = &c->impl;
+    if (!batch || !out || (batch->n_pairs && (!batch->q_off || !batch->q_len || !batch->t_off || !batch->t_len ||
+                                               !out->aln || (!batch->seq && batch->seq_bytes))))
+        return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena pointer");
+    if (!valid_engine(engine)) return phr::set_error(ctx, PHR_ERR_ARG, "unknown engine");
+    out->cigar_used = 0;
+    const uint64_t n = batch->n_pairs;
+    if (n == 0) return PHR_OK;
+    uint64_t sum_qt = 0;
+    for (uint64_t i = 0; i < n; ++i) sum_qt += static_cast<uint64_t>(batch->q_len[i]) + batch->t_len[i];
+    // device output: alignments + worst-case packed text, in the io arena after the inputs
+    const uint64_t text_cap = std::min<uint64_t>(out->cigar_capacity, 2 * sum_qt + 16 * n);
+    const size_t extra = n * sizeof(phr_alignment) + text_cap + 1024;
+    phr::DevPairs dp;
+    phr_status s = upload_pairs(ctx, batch, &dp, &sum_qt, extra);
+    if (s != PHR_OK) return s;
+    phr::DevResults r;
+    r.aln = static_cast<phr_alignment*>(ctx->io.take(n * sizeof(phr_alignment)));
+    r.cigar = static_cast<char*>(ctx->io.take(text_cap + 16));
+    r.cigar_capacity = text_cap;
+    s = phr::run_extend(ctx, engine, dp, costs, &r, sum_qt);
+    if (s != PHR_OK) return s;
+    if (r.cigar_used > out->cigar_capacity)
+        return phr::set_error(ctx, PHR_ERR_CAPACITY, "CIGAR arena too small");
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(out->aln, r.aln, n * sizeof(phr_alignment), cudaMemcpyDeviceToHost, ctx->stream));
+    if (r.cigar_used)
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(out->cigar, r.cigar, r.cigar_used, cudaMemcpyDeviceToHost, ctx->stream));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    out->cigar_used = r.cigar_used;
+    return PHR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t phr_abi_version(void) { return PHR_ABI_VERSION; }
+
+const char* phr_status_string(phr_status s) {
+    switch (s) {
+        case PHR_OK: return "ok";
+        case PHR_INVALID_INPUT: return "invalid input (seed beyond sequence end)";
+        case PHR_ALIGNMENT_FAILED: return "alignment failed (search exhausted)";
+        case PHR_ERR_OOM: return "out of device memory";
+        case PHR_ERR_TIMEOUT: return "device wait timed out";
+        case PHR_ERR_CUDA: return "CUDA error";
+        case PHR_ERR_ARG: return "bad argument";
+        case PHR_ERR_CAPACITY: return "output arena too small";
+        case PHR_ERR_STATE: return "call out of order";
+    }
+    return "unknown status";
+}
+
+phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out) {
+    if (!out) return PHR_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PHR_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return PHR_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return PHR_ERR_CUDA;
+    phr_ctx* c = new (std::nothrow) phr_ctx();
+    if (!c) return PHR_ERR_OOM;
+    Ctx* ctx = &c->impl;
+    ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PHR_ERR_CUDA;
+    }
+    if (cfg && cfg->workspace_bytes) ctx->scratch_budget = cfg->workspace_bytes;
+    if (cfg && cfg->tune_file_enable) {
+        ctx->tune_file_enable = true;
+        ctx->tune_file = cfg->tune_file ? cfg->tune_file : "phraya_b200_tune.txt";
+    }
+    *out = c;
+    return PHR_OK;
+}
+
+void phr_ctx_destroy(phr_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->impl.device);
+    cudaStreamSynchronize(c->impl.stream);
+    delete c;
+}
+
+const char* phr_ctx_last_error(const phr_ctx* c) { return c ? c->impl.last_error.c_str() : "null context"; }
+
+uint64_t phr_ctx_kernel_launches(const phr_ctx* c) { return c ? c->impl.launches.load() : 0; }
+
+phr_status phr_extend_batch(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                            phr_result_arena* out) {
+    if (check_ctx(c) != PHR_OK) return PHR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->impl.mu);
+    cudaSetDevice(c->impl.device);
+    return extend_host(c, engine, batch, costs, out);
+}
+
+phr_status phr_extend_batch_device(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch,
+                                   phr_affine_costs costs, phr_result_arena* out) {
+    if (check_ctx(c) != PHR_OK) return PHR_ERR_ARG;
+    Ctx* ctx = &c->impl;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!batch || !out) return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena");
+    if (!valid_engine(engine)) return phr::set_error(ctx, PHR_ERR_ARG, "unknown engine");
+    // sum of lengths (device arrays): one reduction pass on the host copy of lengths
+    const uint64_t n = batch->n_pairs;
+    out->cigar_used = 0;
+    if (n == 0) return PHR_OK;
+    std::vector<uint32_t> ql(n), tl(n);
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(ql.data(), batch->q_len, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(tl.data(), batch->t_len, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    uint64_t sum_qt = 0;
+    for (uint64_t i = 0; i < n; ++i) sum_qt += static_cast<uint64_t>(ql[i]) + tl[i];
+    phr::DevPairs dp;
+    dp.n = n;
+    dp.seq = batch->seq;
+    dp.seq_bytes = batch->seq_bytes;
+    dp.q_off = batch->q_off;
+    dp.q_len = batch->q_len;
+    dp.t_off = batch->t_off;
+    dp.t_len = batch->t_len;
+    dp.q_seed = batch->q_seed;
+    dp.t_seed = batch->t_seed;
+    phr::DevResults r;
+    r.aln = out->aln;
+    r.cigar = out->cigar;
+    r.cigar_capacity = out->cigar_capacity;
+    phr_status s = phr::run_extend(ctx, engine, dp, costs, &r, sum_qt);
+    out->cigar_used = r.cigar_used;
+    return s;
+}
+
+phr_status phr_extend_percall(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                              phr_result_arena* out) {
+    if (check_ctx(c) != PHR_OK) return PHR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->impl.mu);
+    cudaSetDevice(c->impl.device);
+    Ctx* ctx = &c->impl;
+    if (!batch || !out) return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena");
+    uint64_t used = 0;
+    for (uint64_t i = 0; i < batch->n_pairs; ++i) {
+        phr_pair_batch one = *batch;
+        one.n_pairs = 1;
+        one.q_off = batch->q_off + i;
+        one.q_len = batch->q_len + i;
+        one.t_off = batch->t_off + i;
+        one.t_len = batch->t_len + i;
+        one.q_seed = batch->q_seed ? batch->q_seed + i : nullptr;
+        one.t_seed = batch->t_seed ? batch->t_seed + i : nullptr;
+        phr_result_arena o;
+        o.aln = out->aln + i;
+        o.cigar = out->cigar + used;
+        o.cigar_capacity = out->cigar_capacity - used;
+        o.cigar_used = 0;
+        phr_status s = extend_host(c, engine, &one, costs, &o);
+        if (s != PHR_OK) return s;
+        out->aln[i].cigar_off += used;
+        used += o.cigar_used;
+    }
+    out->cigar_used = used;
+    return PHR_OK;
+}
+
+}  // extern "C"

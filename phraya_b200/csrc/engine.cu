@@ -1,0 +1,668 @@
+// engine.cu -- extension batch driver: pair preparation (suffixes, 2-bit packing),
+// length-bucketed task lists, persistent-kernel launches with overflow redo passes,
+// and packing of the CIGAR text into the caller's arena.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace phr {
+
+// ---------------------------------------------------------------------------
+// DeviceArena
+// ---------------------------------------------------------------------------
+cudaError_t DeviceArena::reserve(size_t need) {
+    if (need <= cap) return cudaSuccess;
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    size_t want = std::max(need + need / 4, static_cast<size_t>(64) << 20);
+    cudaError_t e = cudaMalloc(&base, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc(&base, need);
+        if (e != cudaSuccess) {
+            base = nullptr;
+            return e;
+        }
+        want = need;
+    }
+    cap = want;
+    used = 0;
+    return cudaSuccess;
+}
+
+void* DeviceArena::take(size_t bytes, size_t align) {
+    size_t off = (used + align - 1) / align * align;
+    if (off + bytes > cap) return nullptr;
+    used = off + bytes;
+    return base + off;
+}
+
+DeviceArena::~DeviceArena() {
+    if (base) cudaFree(base);
+}
+
+Ctx::~Ctx() {
+    if (d_counters) cudaFree(d_counters);
+    if (h_pinned) cudaFreeHost(h_pinned);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+phr_status set_error(Ctx* ctx, phr_status st, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return st;
+}
+
+phr_status cuda_status(Ctx* ctx, cudaError_t e, const char* what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return set_error(ctx, PHR_ERR_OOM, msg);
+    return set_error(ctx, PHR_ERR_CUDA, msg);
+}
+
+namespace {
+
+constexpr uint32_t kInvalidKey = 0xFFFFFFFFu;
+
+__device__ __forceinline__ int next_pow2_cap32(int v) {
+    int g = 1;
+    while (g < v && g < 32) g <<= 1;
+    return g;
+}
+
+struct PrepParams {
+    DevPairs in;
+    int32_t engine;
+    phr_affine_costs costs;
+    PairDesc* desc;
+    PairOut* out;
+    uint64_t* w2;      // 2-bit words per pair -> scanned in place to offsets
+    uint64_t* wb;      // byte words per pair
+    uint64_t* tb;      // text bound per pair
+};
+
+// Suffix lengths, seed validation, arena sizes. One thread per pair.
+__global__ void prep_sizes_kernel(PrepParams P) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= P.in.n) return;
+    const uint32_t ql = P.in.q_len[i], tl = P.in.t_len[i];
+    uint32_t qs = P.in.q_seed ? P.in.q_seed[i] : 0, ts = P.in.t_seed ? P.in.t_seed[i] : 0;
+    if (P.engine == PHR_ENGINE_MYERS_GLOBAL) qs = ts = 0;
+    PairDesc d = {};
+    const bool invalid = qs > ql || ts > tl;
+    d.qs = static_cast<int32_t>(qs);
+    d.ts = static_cast<int32_t>(ts);
+    d.qn = invalid ? 0 : static_cast<int32_t>(ql - qs);
+    d.tn = invalid ? 0 : static_cast<int32_t>(tl - ts);
+    d.trivial = (invalid || d.qn == 0 || d.tn == 0) ? 1 : 0;
+    d.mode = 0;
+    P.desc[i] = d;
+    PairOut o = {};
+    o.status = invalid ? PHR_INVALID_INPUT : -1;  // -1: not yet produced
+    P.out[i] = o;
+    const uint64_t qn = d.qn, tn = d.tn;
+    P.w2[i] = d.trivial ? 0 : (qn + 15) / 16 + 4 + (tn + 15) / 16 + 4;
+    P.wb[i] = d.trivial ? 0 : (qn + 3) / 4 + 4 + (tn + 3) / 4 + 4;
+    P.tb[i] = 2 * (qn + tn) + 16;
+}
+
+__device__ __forceinline__ uint32_t code2(uint8_t b, bool& pure) {
+    switch (b) {
+        case 'A': return 0;
+        case 'C': return 1;
+        case 'G': return 2;
+        case 'T': return 3;
+        default: pure = false; return 0;
+    }
+}
+
+// Writes "<n><op>" at p, returns its length.
+__device__ uint32_t write_count_op(char* p, uint32_t n, char op) {
+    const uint32_t nd = ndigits(n);
+    for (int d = static_cast<int>(nd) - 1; d >= 0; --d) {
+        p[d] = static_cast<char>('0' + n % 10);
+        n /= 10;
+    }
+    p[nd] = op;
+    return nd + 1;
+}
+
+struct PackParams {
+    DevPairs in;
+    int32_t engine;
+    phr_affine_costs costs;
+    PairDesc* desc;
+    PairOut* out;
+    const uint64_t* w2_off;
+    const uint64_t* wb_off;
+    const uint64_t* text_off;
+    uint32_t* arena2;
+    uint32_t* arenab;
+    char* text;
+    uint32_t* keys;
+    uint32_t* vals;
+    int wfa_g_short, wfa_g_long;
+};
+
+// 2-bit packing (16 bases per word) of both suffixes; a pair holding any byte other
+// than A/C/G/T is also copied word-aligned to the byte arena and runs the byte path.
+// Trivial pairs (an empty suffix) get their final result here. One warp per pair.
+__global__ void pack_kernel(PackParams P) {
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= P.in.n) return;
+    const uint64_t i = warp;
+    PairDesc d = P.desc[i];
+    if (d.trivial) {
+        if (lane == 0) {
+            PairOut o = P.out[i];
+            P.keys[i] = kInvalidKey;
+            P.vals[i] = static_cast<uint32_t>(i);
+            if (o.status == PHR_INVALID_INPUT) {
+                o.ed = 0;
+                o.t_consumed = 0;
+                o.text_len = 0;
+                P.out[i] = o;
+                return;
+            }
+            char* t = P.text + P.text_off[i];
+            uint32_t len = 0;
+            o.status = PHR_OK;
+            o.affine_score = 0;
+            const int qn = d.qn, tn = d.tn;
+            if (P.engine == PHR_ENGINE_MYERS_GLOBAL) {
+                if (qn == 0) {
+                    o.ed = tn;
+                    if (tn > 0) len = write_count_op(t, tn, 'I');
+                } else {
+                    o.ed = qn;
+                    len = write_count_op(t, qn, 'D');
+                }
+                o.t_consumed = tn;
+            } else if (qn == 0) {
+                o.ed = 0;  // wfa_simd.rs:194-203 / :365-367 / :592-601, :3793-3795
+                o.t_consumed = 0;
+            } else {      // tn == 0: every query base is query-extra
+                o.ed = qn;
+                len = write_count_op(t, qn, 'D');
+                o.t_consumed = 0;
+                if (P.engine == PHR_ENGINE_WFA_AFFINE) o.affine_score = P.costs.gap_open + qn * P.costs.gap_extend;
+            }
+            o.n_runs = len ? 1 : 0;
+            o.text_len = len;
+            P.out[i] = o;
+        }
+        return;
+    }
+    const uint8_t* qsrc = P.in.seq + P.in.q_off[i] + d.qs;
+    const uint8_t* tsrc = P.in.seq + P.in.t_off[i] + d.ts;
+    const uint64_t w2 = P.w2_off[i];
+    const uint64_t q2w = (d.qn + 15) / 16 + 4;
+    bool pure = true;
+    for (int side = 0; side < 2; ++side) {
+        const uint8_t* src = side ? tsrc : qsrc;
+        const int len = side ? d.tn : d.qn;
+        uint32_t* dst = P.arena2 + w2 + (side ? q2w : 0);
+        const int nw = (len + 15) / 16;
+        for (int w = lane; w < nw; w += 32) {
+            uint32_t word = 0;
+            const int p0 = w * 16;
+            const int lim = min(16, len - p0);
+            for (int b = 0; b < lim; ++b) word |= code2(src[p0 + b], pure) << (2 * b);
+            dst[w] = word;
+        }
+    }
+    pure = __all_sync(PHR_FULL_MASK, pure);
+    if (pure) {
+        d.mode = 0;
+        d.q_word = w2;
+        d.t_word = w2 + q2w;
+    } else {
+        const uint64_t wb = P.wb_off[i];
+        const uint64_t qbw = (d.qn + 3) / 4 + 4;
+        for (int side = 0; side < 2; ++side) {
+            const uint8_t* src = side ? tsrc : qsrc;
+            const int len = side ? d.tn : d.qn;
+            uint32_t* dst = P.arenab + wb + (side ? qbw : 0);
+            const int nw = (len + 3) / 4;
+            for (int w = lane; w < nw; w += 32) {
+                uint32_t word = 0;
+                const int p0 = w * 4;
+                const int lim = min(4, len - p0);
+                for (int b = 0; b < lim; ++b) word |= static_cast<uint32_t>(src[p0 + b]) << (8 * b);
+                dst[w] = word;
+            }
+        }
+        d.mode = 1;
+        d.q_word = wb;
+        d.t_word = wb + qbw;
+    }
+    if (lane == 0) {
+        P.desc[i] = d;
+        int G;
+        uint32_t len;
+        if (P.engine == PHR_ENGINE_MYERS_FIT || P.engine == PHR_ENGINE_MYERS_GLOBAL) {
+            G = next_pow2_cap32((d.qn + 63) / 64);
+            len = static_cast<uint32_t>(d.tn) * (static_cast<uint32_t>((d.qn + 63) / 64));
+        } else {
+            G = (d.qn + d.tn < 1024) ? P.wfa_g_short : P.wfa_g_long;
+            len = static_cast<uint32_t>(d.qn + d.tn);
+        }
+        const uint32_t glog = static_cast<uint32_t>(__ffs(G) - 1);
+        const uint32_t lk = 0x0FFFFFFFu - min(len, 0x0FFFFFFFu);  // longest first within a bucket
+        P.keys[i] = (static_cast<uint32_t>(d.mode) << 31) | (glog << 28) | lk;
+        P.vals[i] = static_cast<uint32_t>(i);
+    }
+}
+
+struct TaskBuild {
+    const uint32_t* keys;      // sorted
+    const uint32_t* order;     // sorted pair ids
+    uint64_t n;
+    uint32_t* head;            // scratch: segment head positions
+    uint32_t* flag;
+    uint32_t* tidx;
+    uint32_t* task_first;
+    uint8_t* task_count;
+    uint8_t* task_group;
+    uint32_t* ranges;          // {0, split, split, n_tasks}
+    uint32_t* split_min;
+    const PairDesc* desc;
+    int32_t engine;
+    int32_t band_base;
+    unsigned long long* need_max;
+};
+
+__device__ __forceinline__ int key_group(uint32_t k) { return 1 << ((k >> 28) & 7); }
+__device__ __forceinline__ uint32_t key_seg(uint32_t k) { return k >> 28; }
+
+__global__ void task_head_kernel(TaskBuild T) {
+    const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (p >= T.n) return;
+    const uint32_t k = T.keys[p];
+    T.head[p] = (p == 0 || key_seg(T.keys[p - 1]) != key_seg(k)) ? static_cast<uint32_t>(p) : 0u;
+}
+
+__global__ void task_flag_kernel(TaskBuild T) {
+    const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (p >= T.n) return;
+    const uint32_t k = T.keys[p];
+    const uint32_t per = 32 / key_group(k);
+    T.flag[p] = (k != kInvalidKey && ((p - T.head[p]) % per) == 0) ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint64_t myers_need_est(int m, int n, int G, int band_base) {
+    const int nb = (m + 63) >> 6;
+    int E = min(band_base + abs(m - n) + (m >> 3), max(m, n));
+    int W = min((2 * (E + 2) + 1 + 63) / 64 + 1, nb);
+    uint64_t need = ((static_cast<uint64_t>(n) * W * 32) + 15) & ~15ull;
+    if (nb > G) need += (static_cast<uint64_t>(n) + 15) & ~15ull;
+    need += (static_cast<uint64_t>(m + n + 2) * 4 + 15) & ~15ull;
+    return need;
+}
+
+__device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool affine) {
+    const uint64_t L = static_cast<uint64_t>(qn + tn);
+    return affine ? (160ull << 10) + 512ull * L : (32ull << 10) + 64ull * L;
+}
+
+__global__ void task_fill_kernel(TaskBuild T) {
+    const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (p >= T.n || !T.flag[p]) return;
+    const uint32_t k = T.keys[p];
+    const int G = key_group(k);
+    const uint32_t per = 32 / G;
+    uint32_t cnt = 0;
+    uint64_t need = 0, region = 0;
+    for (uint32_t c = 0; c < per && p + c < T.n; ++c) {
+        const uint32_t kc = T.keys[p + c];
+        if (kc == kInvalidKey || key_seg(kc) != key_seg(k)) break;
+        const PairDesc d = T.desc[T.order[p + c]];
+        if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
+            need += myers_need_est(d.qn, d.tn, G, T.band_base);
+        else
+            region = max(region, wfa_region_est(d.qn, d.tn, T.engine == PHR_ENGINE_WFA_AFFINE));
+        ++cnt;
+    }
+    if (T.engine != PHR_ENGINE_MYERS_FIT && T.engine != PHR_ENGINE_MYERS_GLOBAL) need = region * per;
+    const uint32_t t = T.tidx[p];
+    T.task_first[t] = static_cast<uint32_t>(p);
+    T.task_count[t] = static_cast<uint8_t>(cnt);
+    T.task_group[t] = static_cast<uint8_t>(G);
+    atomicMax(T.need_max, static_cast<unsigned long long>(need));
+    if ((k >> 31) & 1) atomicMin(T.split_min, t);
+}
+
+__global__ void task_finalize_kernel(TaskBuild T) {
+    uint32_t nt = 0;
+    if (T.n > 0) nt = T.tidx[T.n - 1] + T.flag[T.n - 1];
+    const uint32_t split = min(*T.split_min, nt);
+    T.ranges[0] = 0;
+    T.ranges[1] = split;
+    T.ranges[2] = split;
+    T.ranges[3] = nt;
+}
+
+// Redo pass task list: one pair per task, in redo order.
+__global__ void redo_tasks_kernel(const uint32_t* redo_list, const uint32_t* redo_count, const PairDesc* desc,
+                                  int32_t engine, int wfa_g_short, int wfa_g_long, uint32_t* task_first,
+                                  uint8_t* task_count, uint8_t* task_group, uint32_t* ranges) {
+    const uint32_t n = *redo_count;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        ranges[0] = 0;
+        ranges[1] = n;
+    }
+    if (t >= n) return;
+    const PairDesc d = desc[redo_list[t]];
+    int G;
+    if (engine == PHR_ENGINE_MYERS_FIT || engine == PHR_ENGINE_MYERS_GLOBAL)
+        G = next_pow2_cap32((d.qn + 63) / 64);
+    else
+        G = (d.qn + d.tn < 1024) ? wfa_g_short : wfa_g_long;
+    task_first[t] = t;
+    task_count[t] = 1;
+    task_group[t] = static_cast<uint8_t>(G);
+}
+
+struct FinishParams {
+    uint64_t n;
+    int32_t engine;
+    const PairDesc* desc;
+    const PairOut* out;
+    const uint64_t* text_off;
+    const char* text;
+    uint64_t* cig_off;       // exclusive scan of text_len
+    phr_alignment* aln;
+    char* cigar;
+    uint64_t cigar_capacity;
+    uint32_t* error_flag;
+};
+
+__global__ void text_len_kernel(const PairOut* out, uint64_t n, uint64_t* len) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const PairOut o = out[i];
+    len[i] = (o.status == PHR_OK) ? o.text_len : 0;
+}
+
+// Packs CIGAR text and writes the phr_alignment records. One warp per pair.
+__global__ void finish_kernel(FinishParams F) {
+    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= F.n) return;
+    const uint64_t i = warp;
+    const PairOut o = F.out[i];
+    const PairDesc d = F.desc[i];
+    const uint64_t off = F.cig_off[i];
+    const uint32_t len = (o.status == PHR_OK) ? o.text_len : 0;
+    if (o.status == -1) {
+        if (lane == 0) atomicOr(F.error_flag, 8u);
+        return;
+    }
+    if (off + len <= F.cigar_capacity) {
+        const char* src = F.text + F.text_off[i];
+        for (uint32_t c = lane; c < len; c += 32) F.cigar[off + c] = src[c];
+    } else if (lane == 0) {
+        atomicOr(F.error_flag, 16u);
+    }
+    if (lane == 0) {
+        phr_alignment a;
+        a.status = o.status;
+        a.edit_distance = o.status == PHR_OK ? static_cast<uint32_t>(o.ed) : 0;
+        a.cigar_off = off;
+        a.cigar_len = len;
+        a.affine_score = o.status == PHR_OK ? static_cast<uint32_t>(o.affine_score) : 0;
+        if (F.engine == PHR_ENGINE_MYERS_GLOBAL) {
+            a.query_start = 0;
+            a.query_end = static_cast<uint32_t>(d.qn);
+            a.target_start = 0;
+            a.target_end = static_cast<uint32_t>(d.tn);
+        } else if (o.status == PHR_INVALID_INPUT || o.status == PHR_ALIGNMENT_FAILED) {
+            a.query_start = a.query_end = a.target_start = a.target_end = 0;
+        } else {
+            a.query_start = static_cast<uint32_t>(d.qs);
+            a.query_end = static_cast<uint32_t>(d.qs + d.qn);
+            a.target_start = static_cast<uint32_t>(d.ts);
+            a.target_end = static_cast<uint32_t>(d.ts + o.t_consumed);
+        }
+        F.aln[i] = a;
+    }
+}
+
+__global__ void total_kernel(const uint64_t* off, const uint64_t* len, uint64_t n, uint64_t* total) {
+    *total = n ? off[n - 1] + len[n - 1] : 0;
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned t) { return static_cast<unsigned>((n + t - 1) / t); }
+
+}  // namespace
+
+size_t extend_arena_need(uint64_t n, uint64_t seq_bytes, uint64_t sum_qt) {
+    size_t s = 0;
+    auto add = [&](size_t b) { s += (b + 511) / 256 * 256; };
+    add(n * sizeof(PairDesc));
+    add(n * sizeof(PairOut));
+    add(n * 8 * 3);                       // w2, wb, tb (scanned in place)
+    add(n * 8 * 3);                       // scan outputs
+    add((sum_qt / 16 + 12 * n + 64) * 4);  // 2-bit arena
+    add((sum_qt / 4 + 12 * n + 64) * 4);   // byte arena
+    add(2 * sum_qt + 16 * n + 64);        // text staging
+    add(n * 4 * 4);                       // keys/vals (2x for sort)
+    add(n * 4 * 6);                       // task build scratch
+    add(n * 6);                           // task count/group
+    add(n * 8 * 2);                       // text len + cigar offsets
+    add(n * 4);                           // redo list
+    add(64ull << 20);                     // CUB temp
+    add(4096);
+    return s;
+}
+
+phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affine_costs costs, DevResults* res,
+                      uint64_t sum_qt) {
+    const uint64_t n = in.n;
+    cudaStream_t st = ctx->stream;
+    res->cigar_used = 0;
+    if (n == 0) return PHR_OK;
+    if (n > 0xFFFFFFF0ull) return set_error(ctx, PHR_ERR_ARG, "too many pairs in one batch");
+    DeviceArena& A = ctx->arena;
+    A.reset();
+    PHR_CUDA_TRY(ctx, A.reserve(extend_arena_need(n, in.seq_bytes, sum_qt)));
+    auto take = [&](size_t b) { return A.take(b); };
+    PairDesc* desc = static_cast<PairDesc*>(take(n * sizeof(PairDesc)));
+    PairOut* pout = static_cast<PairOut*>(take(n * sizeof(PairOut)));
+    uint64_t* w2 = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* wb = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* tb = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* w2o = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* wbo = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* tbo = static_cast<uint64_t*>(take(n * 8));
+    // per sequence ceil(len/16)+4 (2-bit) / ceil(len/4)+4 (byte) words: <= len/16 + 5 per sequence
+    uint32_t* arena2 = static_cast<uint32_t*>(take((sum_qt / 16 + 12 * n + 64) * 4));
+    uint32_t* arenab = static_cast<uint32_t*>(take((sum_qt / 4 + 12 * n + 64) * 4));
+    char* text = static_cast<char*>(take(2 * sum_qt + 16 * n + 64));
+    uint32_t* keys = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* vals = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* keys_s = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* order = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* head = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* head_s = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* flag = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* tidx = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* task_first = static_cast<uint32_t*>(take(n * 4));
+    uint32_t* redo_list = static_cast<uint32_t*>(take(n * 4));
+    uint8_t* task_count = static_cast<uint8_t*>(take(n));
+    uint8_t* task_group = static_cast<uint8_t*>(take(n));
+    uint64_t* tlen = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* cigoff = static_cast<uint64_t*>(take(n * 8));
+    // counters: [0..3] ranges, [4] split_min, [5] queue head 0, [6] queue head 1,
+    // [7] redo count, [8..9] need max (u64), [10] error flag, [12..13] total (u64), [14..17] redo ranges
+    uint32_t* cnt = static_cast<uint32_t*>(take(256));
+    if (!cnt) return set_error(ctx, PHR_ERR_OOM, "device arena exhausted");
+    unsigned long long* need_max = reinterpret_cast<unsigned long long*>(cnt + 8);
+    uint64_t* total = reinterpret_cast<uint64_t*>(cnt + 12);
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, 256, st));
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 4, 0xFF, 4, st));
+
+    // CUB temp sizes
+    size_t t_sort = 0, t_scan = 0, t_max = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, keys, keys_s, vals, order, static_cast<int>(n), 0, 32, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, t_scan, w2, w2o, static_cast<int>(n), st);
+    cub::DeviceScan::InclusiveScan(nullptr, t_max, head, head_s, cub::Max(), static_cast<int>(n), st);
+    size_t t_scan32 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t_scan32, flag, tidx, static_cast<int>(n), st);
+    const size_t t_need = std::max({t_sort, t_scan, t_max, t_scan32});
+    void* tmp = take(t_need);
+    if (!tmp) return set_error(ctx, PHR_ERR_OOM, "device arena exhausted (cub)");
+
+    const unsigned T = 256;
+    PrepParams pp{in, engine, costs, desc, pout, w2, wb, tb};
+    prep_sizes_kernel<<<blocks_for(n, T), T, 0, st>>>(pp);
+    ++ctx->launches;
+    size_t tn_ = t_need;
+    cub::DeviceScan::ExclusiveSum(tmp, tn_, w2, w2o, static_cast<int>(n), st);
+    tn_ = t_need;
+    cub::DeviceScan::ExclusiveSum(tmp, tn_, wb, wbo, static_cast<int>(n), st);
+    tn_ = t_need;
+    cub::DeviceScan::ExclusiveSum(tmp, tn_, tb, tbo, static_cast<int>(n), st);
+
+    PackParams pk{in, engine, costs, desc, pout, w2o, wbo, tbo, arena2, arenab, text, keys, vals,
+                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long};
+    pack_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(pk);
+    ++ctx->launches;
+    tn_ = t_need;
+    cub::DeviceRadixSort::SortPairs(tmp, tn_, keys, keys_s, vals, order, static_cast<int>(n), 0, 32, st);
+
+    TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, desc,
+                  engine, ctx->tune.myers_band_base, need_max};
+    task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    tn_ = t_need;
+    cub::DeviceScan::InclusiveScan(tmp, tn_, head, head_s, cub::Max(), static_cast<int>(n), st);
+    tbp.head = head_s;
+    task_flag_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    tn_ = t_need;
+    cub::DeviceScan::ExclusiveSum(tmp, tn_, flag, tidx, static_cast<int>(n), st);
+    task_fill_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    task_finalize_kernel<<<1, 1, 0, st>>>(tbp);
+    ctx->launches += 4;
+
+    // slot size for the main pass
+    uint64_t h_need = 0;
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_need, need_max, 8, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    PHR_CUDA_TRY(ctx, cudaGetLastError());
+
+    const bool is_myers = engine == PHR_ENGINE_MYERS_FIT || engine == PHR_ENGINE_MYERS_GLOBAL;
+    ExtendParams P{};
+    P.desc = desc;
+    P.out = pout;
+    P.packed2 = arena2;
+    P.bytes = arenab;
+    P.text = text;
+    P.text_off = tbo;
+    P.scratch = nullptr;
+    P.redo_list = redo_list;
+    P.redo_count = cnt + 7;
+    P.redo_need_max = need_max;
+    P.engine = engine;
+    P.full_band = 0;
+    P.band_base = ctx->tune.myers_band_base;
+    P.costs = costs;
+    P.error_flag = cnt + 10;
+
+    const int block = ctx->tune.block_threads;
+    auto launch_pass = [&](const uint32_t* ord, const uint32_t* tfirst, const uint8_t* tcount, const uint8_t* tgroup,
+                           const uint32_t* range0, const uint32_t* range1, uint64_t slot, int full_band) -> phr_status {
+        slot = std::max<uint64_t>((slot + 255) & ~255ull, 4096);
+        // grid: resident blocks per SM, shrunk to the scratch budget
+        uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * 4;
+        const uint64_t warps_per_block = block / 32;
+        while (grid > 1 && grid * warps_per_block * slot > ctx->scratch_budget) grid = (grid + 1) / 2;
+        PHR_CUDA_TRY(ctx, ctx->scratch.reserve(grid * warps_per_block * slot));
+        P.scratch = reinterpret_cast<uint8_t*>(ctx->scratch.base);
+        P.slot_bytes = slot;
+        P.full_band = full_band;
+        P.tasks.order = ord;
+        P.tasks.task_first = tfirst;
+        P.tasks.task_count = tcount;
+        P.tasks.task_group = tgroup;
+        PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 5, 0, 8, st));
+        P.tasks.range = range0;
+        P.queue_head = cnt + 5;
+        if (is_myers)
+            launch_myers(P, static_cast<int>(grid), block, st);
+        else if (engine == PHR_ENGINE_WFA_LINEAR)
+            launch_wfa_linear(P, static_cast<int>(grid), block, st);
+        else
+            launch_wfa_affine(P, static_cast<int>(grid), block, st);
+        P.tasks.range = range1;
+        P.queue_head = cnt + 6;
+        if (is_myers)
+            launch_myers_bytes(P, static_cast<int>(grid), block, st);
+        else if (engine == PHR_ENGINE_WFA_LINEAR)
+            launch_wfa_linear_bytes(P, static_cast<int>(grid), block, st);
+        else
+            launch_wfa_affine_bytes(P, static_cast<int>(grid), block, st);
+        ctx->launches += 2;
+        PHR_CUDA_TRY(ctx, cudaGetLastError());
+        return PHR_OK;
+    };
+
+    phr_status s = launch_pass(order, task_first, task_count, task_group, cnt + 0, cnt + 2, h_need, 0);
+    if (s != PHR_OK) return s;
+
+    // overflow redo passes: each pair that did not fit its slot (or, for Myers, whose
+    // edit distance left the stored band) runs again alone with the room it asked for
+    uint32_t* rlist = redo_list;
+    uint32_t* rlist2 = head;  // reuse: free after task build
+    for (int pass = 0; pass < 12; ++pass) {
+        uint32_t h_redo[4] = {0, 0, 0, 0};
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_redo, cnt + 7, 4, cudaMemcpyDeviceToHost, st));
+        uint64_t h_need2 = 0;
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_need2, need_max, 8, cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        if (h_redo[0] == 0) break;
+        if (pass == 11) return set_error(ctx, PHR_ERR_CAPACITY, "extension did not fit after repeated redo passes");
+        if (h_need2 > ctx->scratch_budget)
+            return set_error(ctx, PHR_ERR_OOM, "a single pair needs more scratch than the workspace budget");
+        // tasks from the redo list; swap lists so the pass can append fresh overflows
+        redo_tasks_kernel<<<blocks_for(h_redo[0], T), T, 0, st>>>(rlist, cnt + 7, desc, engine,
+                                                                 ctx->tune.wfa_group_short, ctx->tune.wfa_group_long,
+                                                                 task_first, task_count, task_group, cnt + 14);
+        ++ctx->launches;
+        // byte-mode and 2-bit pairs share this list: both launches walk all of it
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cnt + 16, cnt + 14, 8, cudaMemcpyDeviceToDevice, st));
+        PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 7, 0, 4, st));
+        P.redo_list = rlist2;
+        s = launch_pass(rlist, task_first, task_count, task_group, cnt + 14, cnt + 16, h_need2, 1);
+        if (s != PHR_OK) return s;
+        std::swap(rlist, rlist2);
+    }
+
+    // pack CIGAR text
+    text_len_kernel<<<blocks_for(n, T), T, 0, st>>>(pout, n, tlen);
+    tn_ = t_need;
+    cub::DeviceScan::ExclusiveSum(tmp, tn_, tlen, cigoff, static_cast<int>(n), st);
+    total_kernel<<<1, 1, 0, st>>>(cigoff, tlen, n, total);
+    uint64_t h_total = 0;
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_total, total, 8, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (h_total > res->cigar_capacity)
+        return set_error(ctx, PHR_ERR_CAPACITY, "CIGAR arena too small: need " + std::to_string(h_total) + " bytes");
+    FinishParams F{n, engine, desc, pout, tbo, text, cigoff, res->aln, res->cigar, res->cigar_capacity, cnt + 10};
+    finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
+    ctx->launches += 3;
+    uint32_t h_err = 0;
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_err, cnt + 10, 4, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    PHR_CUDA_TRY(ctx, cudaGetLastError());
+    if (h_err) return set_error(ctx, PHR_ERR_CUDA, "internal consistency check failed (flags " + std::to_string(h_err) + ")");
+    res->cigar_used = h_total;
+    return PHR_OK;
+}
+
+}  // namespace phr

@@ -1,0 +1,98 @@
+// engine.cuh -- host-side runtime of the phraya B200 engine: context, device arena,
+// extension batch driver. Shared by api.cu (C ABI) and pipeline.cu (align_read).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace phr {
+
+// Bump allocator over one growable device buffer. Reset per call; grown (free +
+// cudaMalloc) only between calls, when a call's precomputed need exceeds capacity.
+struct DeviceArena {
+    char* base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+    cudaError_t reserve(size_t need);
+    void reset() { used = 0; }
+    void* take(size_t bytes, size_t align = 256);
+    ~DeviceArena();
+};
+
+// Tunables of one engine; filled from the autotuner cache when present.
+struct EngineTune {
+    int wfa_group_short = 16;    // lanes per pair for WFA pairs with qn+tn < 1024
+    int wfa_group_long = 32;
+    int myers_band_base = 64;
+    int block_threads = 256;
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    DeviceArena arena;       // per-call temporaries
+    DeviceArena scratch;     // per-warp slots of the persistent kernels
+    DeviceArena io;          // device copies of host inputs / outputs
+    size_t scratch_budget = 8ull << 30;
+    std::string last_error;
+    std::atomic<uint64_t> launches{0};
+    EngineTune tune;
+    std::string tune_file;
+    bool tune_file_enable = false;
+    std::mutex mu;
+    uint32_t* d_counters = nullptr;   // small device scratch for counters (pinned size)
+    void* h_pinned = nullptr;         // small pinned host buffer for D2H of counters
+    ~Ctx();
+};
+
+// Device-resident description of a pair batch (pointers into device memory).
+struct DevPairs {
+    uint64_t n = 0;
+    const uint8_t* seq = nullptr;
+    uint64_t seq_bytes = 0;
+    const uint64_t* q_off = nullptr;
+    const uint32_t* q_len = nullptr;
+    const uint64_t* t_off = nullptr;
+    const uint32_t* t_len = nullptr;
+    const uint32_t* q_seed = nullptr;
+    const uint32_t* t_seed = nullptr;
+};
+
+// Device-resident output of a pair batch.
+struct DevResults {
+    phr_alignment* aln = nullptr;  // n entries (device)
+    char* cigar = nullptr;         // packed text (device)
+    uint64_t cigar_capacity = 0;
+    uint64_t cigar_used = 0;       // written (host value) by run_extend
+};
+
+// Runs `engine` over the device batch, writing device results. Synchronizes the
+// context stream before returning (needed to size the packed CIGAR output).
+phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& pairs, phr_affine_costs costs,
+                      DevResults* out, uint64_t sum_qt_len);
+
+// Upper bound of the device arena bytes run_extend needs for a batch.
+size_t extend_arena_need(uint64_t n, uint64_t seq_bytes, uint64_t sum_qt_len);
+
+phr_status set_error(Ctx* ctx, phr_status st, const std::string& msg);
+phr_status cuda_status(Ctx* ctx, cudaError_t e, const char* what);
+
+#define PHR_CUDA_TRY(ctx, expr)                                     \
+    do {                                                            \
+        cudaError_t _e = (expr);                                    \
+        if (_e != cudaSuccess) return ::phr::cuda_status(ctx, _e, #expr); \
+    } while (0)
+
+// Extra launchers (byte-mode instantiations) defined in myers.cu / wfa.cu.
+void launch_myers_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st);
+void launch_wfa_linear_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st);
+void launch_wfa_affine_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st);
+
+}  // namespace phr

@@ -1,0 +1,706 @@
+// wfa.cu -- wavefront alignment, linear and gap-affine, with traceback (sm_100a).
+//
+// Semantics restated from phraya-align/src/wfa_simd.rs:
+//   linear   fill_wfa :231-345, fill_wfa_fitting_impl :360-482, fitting_end_k :940-955,
+//            traceback_wfa_with_tend :959-1041 / traceback_wfa :1044-1130
+//   affine   fill_wfa_affine_generic :581-779, affine_pos_valid :563-569,
+//            affine_traceback :785-886, levenshtein_from_cigar :893-908,
+//            fill_wfa_affine_fitting_impl :919-935
+//
+// GPU design. One pair per group of G lanes; the diagonals of a wavefront are dealt to
+// the group's lanes round-robin (diagonal k goes to lane (k + tn) mod G, the same lane
+// for every layer and score, so a cell's I/D/M values never cross lanes within a step).
+// Match runs are extended with 16-base (2-bit) or 4-byte word compares (common.cuh lcp).
+//
+// The reference keeps full-width frames (qn+tn+1 diagonals per score). Only cells
+// reachable from the origin can ever be set, so each frame is stored over its
+// reachable band only: linear [-min(s,tn), min(s,qn)] (the reference's own scan
+// range); affine per layer, the union of its source bands shifted by the move, clipped
+// to [-tn, qn]. Cells outside a band are UNSET in the reference too, so every stored
+// value, op code and tie-break is identical.
+//
+// History per cell is what the traceback needs: the post-extension value (input to
+// later scores) and the pre-extension candidate `raw` with its op code. In both
+// tracebacks the match-run start is exactly `raw` (linear: edit_start = pred_pos+1 for
+// ops 1/2 and pred_pos for op 3 == the winning candidate; affine: raw of each m_op).
+#include "kernels.cuh"
+
+namespace phr {
+namespace {
+
+constexpr int32_t UNSET = INT32_MIN;
+
+__device__ __forceinline__ uint64_t align16(uint64_t v) { return (v + 15) & ~15ull; }
+
+template <class S>
+__device__ __forceinline__ const uint32_t* seq_base(const ExtendParams& P, uint64_t word) {
+    return (S::kBits == 2 ? P.packed2 : P.bytes) + word;
+}
+
+// Group-cooperative CIGAR formatting of `nr` reverse-order runs; returns text length.
+__device__ uint32_t format_group(const uint32_t* runs, uint32_t nr, char* out, int G) {
+    const int gl = lane_id() & (G - 1);
+    const uint32_t nrmax = __reduce_max_sync(PHR_FULL_MASK, nr);
+    const uint32_t rounds = (nrmax + G - 1) / G;
+    uint32_t base = 0;
+    for (uint32_t rr = 0; rr < rounds; ++rr) {
+        const uint32_t c = rr * G + gl;
+        uint32_t len = 0, run = 0;
+        if (c < nr) {
+            run = runs[nr - 1 - c];
+            len = ndigits(run >> 2) + 1;
+        }
+        const uint32_t incl = group_incl_scan(len, G);
+        if (c < nr) {
+            char* p = out + base + incl - len;
+            uint32_t v = run >> 2;
+            const uint32_t nd = len - 1;
+            for (int dd = static_cast<int>(nd) - 1; dd >= 0; --dd) {
+                p[dd] = static_cast<char>('0' + v % 10);
+                v /= 10;
+            }
+            p[nd] = op_char(run & 3);
+        }
+        base += __shfl_sync(PHR_FULL_MASK, incl, G - 1, G);
+    }
+    return base;
+}
+
+__device__ __forceinline__ void report_redo(const ExtendParams& P, uint32_t pid, uint64_t need) {
+    const uint32_t k = atomicAdd(P.redo_count, 1u);
+    P.redo_list[k] = pid;
+    atomicMax(P.redo_need_max, static_cast<unsigned long long>(need));
+}
+
+// ===========================================================================
+// Linear WFA
+// ===========================================================================
+// cells stored before frame s: sum_{s'<s} (min(s',qn) + min(s',tn) + 1)
+__device__ __forceinline__ uint64_t tri_min(int64_t s, int64_t x) {  // sum_{s'=0}^{s-1} min(s', x)
+    if (s <= 0) return 0;
+    if (s - 1 <= x) return static_cast<uint64_t>((s - 1) * s / 2);
+    return static_cast<uint64_t>(x * (x + 1) / 2 + (s - 1 - x) * x);
+}
+__device__ __forceinline__ uint64_t lin_base(int64_t s, int64_t qn, int64_t tn) {
+    return static_cast<uint64_t>(s) + tri_min(s, qn) + tri_min(s, tn);
+}
+
+template <class S>
+__device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint32_t pid, bool act, int G,
+                                 uint8_t* region, uint64_t region_bytes) {
+    const int gl = lane_id() & (G - 1);
+    const int qn = act ? d.qn : 0, tn = act ? d.tn : 0;
+    const bool fitting = act && tn > qn + qn / 2 + 10;
+    const uint32_t* qb = seq_base<S>(P, d.q_word);
+    const uint32_t* tb = seq_base<S>(P, d.t_word);
+
+    // region: [runs (qn+tn+2) u32][hv int32 cells][hr u32 cells]
+    uint32_t* runs = reinterpret_cast<uint32_t*>(region);
+    const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
+    const uint64_t cell_cap = region_bytes > runs_bytes ? (region_bytes - runs_bytes) / 8 : 0;
+    int32_t* hv = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* hr = reinterpret_cast<uint32_t*>(hv + cell_cap);
+
+    // largest score whose frames fit: lin_base(s+1) <= cell_cap
+    const int max_s = qn + tn;
+    bool alive = act;
+    bool done = false, overflow = false;
+    int s_end = 0, t_end = 0;
+
+    // ---- s = 0 ----
+    if (alive) {
+        if (lin_base(1, qn, tn) > cell_cap) {
+            overflow = true;
+            alive = false;
+        }
+    }
+    if (alive && gl == 0) {
+        const int32_t v = wfa_extend<S>(qb, qn, tb, tn, 0, 0);
+        hv[0] = v;
+        hr[0] = 0;
+    }
+    __syncwarp();
+    if (alive) {
+        const int32_t v0 = hv[0];
+        if (!fitting) {
+            if (qn - tn == 0 && v0 == qn) {  // wfa_simd.rs:277-283 (perfect match only on diagonal 0)
+                done = true;
+                s_end = 0;
+                t_end = tn;
+            }
+        } else {
+            // fitting_end_k over the only set diagonal k = 0 (t_end = qn)
+            if (qn <= tn && v0 >= qn) {
+                done = true;
+                s_end = 0;
+                t_end = qn;
+            }
+        }
+    }
+    int s = 1;
+    for (;;) {
+        const bool run = alive && !done && s <= max_s;
+        if (!__any_sync(PHR_FULL_MASK, run)) break;
+        int lo = 0, hi = -1;
+        uint64_t base = 0, pbase = 0;
+        int plo = 0, phi = -1;
+        if (run) {
+            lo = -min(s, tn);
+            hi = min(s, qn);
+            plo = -min(s - 1, tn);
+            phi = min(s - 1, qn);
+            base = lin_base(s, qn, tn);
+            pbase = lin_base(s - 1, qn, tn);
+            if (base + static_cast<uint64_t>(hi - lo + 1) > cell_cap) {
+                overflow = true;
+                alive = false;
+            }
+        }
+        const bool go = run && alive;
+        int best_end_k = INT32_MAX;
+        if (go) {
+            // lane gl handles diagonals k with (k + tn) % G == gl
+            int k = lo + ((gl - ((lo + tn) % G)) % G + G) % G;
+            for (; k <= hi; k += G) {
+                int32_t best_pos = UNSET;
+                uint32_t best_op = 0;
+                bool have = false;
+                // candidates in order [mismatch, ins, del]; the LAST maximal one wins
+                if (k >= plo && k <= phi) {
+                    const int32_t pv = hv[pbase + (k - plo)];
+                    if (pv != UNSET) {
+                        best_pos = pv + 1;
+                        best_op = 1;
+                        have = true;
+                    }
+                }
+                if (k > -tn && k - 1 >= plo && k - 1 <= phi) {
+                    const int32_t pv = hv[pbase + (k - 1 - plo)];
+                    if (pv != UNSET) {
+                        const int32_t c = pv + 1;
+                        if (!have || c >= best_pos) {
+                            best_pos = c;
+                            best_op = 2;
+                            have = true;
+                        }
+                    }
+                }
+                if (k < qn && k + 1 >= plo && k + 1 <= phi) {
+                    const int32_t pv = hv[pbase + (k + 1 - plo)];
+                    if (pv != UNSET) {
+                        if (!have || pv >= best_pos) {
+                            best_pos = pv;
+                            best_op = 3;
+                            have = true;
+                        }
+                    }
+                }
+                int32_t val = UNSET;
+                uint32_t aux = 0;
+                if (have) {
+                    const int32_t j = best_pos - k;
+                    if (!(best_pos < 0 || best_pos > qn || j < 0 || j > tn)) {
+                        val = wfa_extend<S>(qb, qn, tb, tn, best_pos, k);
+                        aux = (static_cast<uint32_t>(best_pos) << 2) | best_op;
+                    }
+                }
+                hv[base + (k - lo)] = val;
+                hr[base + (k - lo)] = aux;
+                if (val != UNSET) {
+                    if (!fitting) {
+                        if (k == qn - tn && val >= qn) best_end_k = k;
+                    } else if (k >= qn - tn && k <= qn && val >= qn) {
+                        best_end_k = min(best_end_k, k);
+                    }
+                }
+            }
+        }
+        // reduce the end diagonal over the group (min k = max t_end)
+        int kk = best_end_k;
+        for (int o = 1; o < G; o <<= 1) kk = min(kk, __shfl_xor_sync(PHR_FULL_MASK, kk, o, G));
+        __syncwarp();
+        if (go && kk != INT32_MAX) {
+            done = true;
+            s_end = s;
+            t_end = qn - kk;
+        }
+        if (run) ++s;
+    }
+    const bool failed = act && !done && !overflow;  // loop exhausted: AlignmentFailed
+    if (act && overflow && gl == 0) {
+        // retry with room for twice the scores reached so far (capped at the full search)
+        const int64_t s2 = ::min(static_cast<long long>(max_s) + 1, 2LL * s + 64);
+        const uint64_t need = align16(static_cast<uint64_t>(qn + tn + 2) * 4) + lin_base(s2, qn, tn) * 8 + 64;
+        report_redo(P, pid, need);
+    }
+
+    // ---- traceback (wfa_simd.rs:959-1041), one walk per group ----
+    RunWriter rw;
+    rw.init(runs, static_cast<uint32_t>(qn + tn + 2));
+    const bool trace = act && done;
+    uint32_t n_x = 0, n_gap = 0;
+    if (trace && gl == 0) {
+        int qi = qn, ti = t_end, k = qi - ti, ss = s_end;
+        while (qi > 0 || ti > 0) {
+            if (ss < 0) break;
+            if (ss == 0) {
+                const int mm = min(qi, ti);
+                rw.push(0, static_cast<uint32_t>(mm));
+                qi -= mm;
+                ti -= mm;
+                break;
+            }
+            const int lo = -min(ss, tn);
+            const uint32_t aux = hr[lin_base(ss, qn, tn) + (k - lo)];
+            const uint32_t op = aux & 3;
+            const int32_t edit_start = static_cast<int32_t>(aux >> 2);
+            const int mc = qi - edit_start;
+            if (mc > 0) {
+                rw.push(0, static_cast<uint32_t>(mc));
+                qi -= mc;
+                ti -= mc;
+            }
+            if (op == 1) {
+                rw.push(1, 1);
+                --qi;
+                --ti;
+                ++n_x;
+            } else if (op == 2) {
+                rw.push(3, 1);  // 'D': query advances
+                --qi;
+                ++n_gap;
+                k -= 1;
+            } else if (op == 3) {
+                rw.push(2, 1);  // 'I': target advances
+                --ti;
+                ++n_gap;
+                k += 1;
+            }
+            --ss;
+        }
+        rw.flush();
+    }
+    const uint32_t nr = __shfl_sync(PHR_FULL_MASK, rw.n, lane_id() & ~(G - 1));
+    const bool ovf = __shfl_sync(PHR_FULL_MASK, rw.overflow ? 1 : 0, lane_id() & ~(G - 1)) != 0;
+    __syncwarp();
+    const uint32_t nr_fmt = (trace && !ovf) ? nr : 0;
+    char* out = act ? P.text + P.text_off[pid] : nullptr;
+    const uint32_t tl = format_group(runs, nr_fmt, out, G);
+    if (act && gl == 0) {
+        if (trace && !ovf) {
+            PairOut o;
+            o.status = PHR_OK;
+            o.ed = s_end;
+            o.t_consumed = t_end;
+            o.affine_score = 0;
+            o.n_runs = nr;
+            o.text_len = tl;
+            P.out[pid] = o;
+        } else if (failed) {
+            PairOut o = {};
+            o.status = PHR_ALIGNMENT_FAILED;
+            P.out[pid] = o;
+        } else if (trace && ovf) {
+            atomicOr(P.error_flag, 2u);
+        }
+    }
+}
+
+// ===========================================================================
+// Gap-affine WFA
+// ===========================================================================
+struct LayerBand {
+    int lo, hi;          // empty when lo > hi
+    uint64_t base;       // first cell of this layer/score in the cell arrays
+};
+
+// Frame directory entry per score s: M, I, D bands.
+struct AffDir {
+    LayerBand L[3];
+};
+
+__device__ __forceinline__ bool aff_valid(int32_t pos, int k, int qn, int tn) {
+    if (pos == UNSET || pos < 0 || pos > qn) return false;
+    const int tp = pos - k;
+    return tp >= 0 && tp <= tn;
+}
+
+template <class S>
+__device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint32_t pid, bool act, int G,
+                                 uint8_t* region, uint64_t region_bytes) {
+    const int gl = lane_id() & (G - 1);
+    const int qn = act ? d.qn : 0, tn = act ? d.tn : 0;
+    const bool fitting = act && tn > qn + qn / 2 + 10;
+    const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
+    const uint32_t* qb = seq_base<S>(P, d.q_word);
+    const uint32_t* tb = seq_base<S>(P, d.t_word);
+    const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
+
+    // region: [runs][cells int2 = {value, aux} growing up ...  ... directory growing down]
+    // Directory entry of score s is dir_top[-1 - s]; cells and directory share the space.
+    uint32_t* runs = reinterpret_cast<uint32_t*>(region);
+    const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
+    const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
+    int2* cells = reinterpret_cast<int2*>(region + runs_bytes);
+    AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + (rest / sizeof(AffDir)) * sizeof(AffDir));
+    const uint64_t dir_cap = rest / sizeof(AffDir);
+    const uint64_t cell_cap = rest / 8;
+    auto dir_at = [&](int64_t sc) -> AffDir& { return dir_top[-1 - sc]; };
+    auto fits = [&](uint64_t ncells, int64_t nscores) -> bool {
+        return ncells * 8 + static_cast<uint64_t>(nscores) * sizeof(AffDir) <= rest;
+    };
+
+    bool alive = act;
+    bool done = false, overflow = false;
+    int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
+    uint64_t used = 0;
+
+    if (alive && (dir_cap < 1 || cell_cap < 1 || !fits(1, 1))) {
+        overflow = true;
+        alive = false;
+    }
+    // ---- s = 0: m0[0] = extend(0, 0) ----
+    if (alive && gl == 0) {
+        AffDir e;
+        e.L[0].lo = 0;
+        e.L[0].hi = 0;
+        e.L[0].base = 0;
+        e.L[1].lo = 1;
+        e.L[1].hi = 0;
+        e.L[1].base = 1;
+        e.L[2].lo = 1;
+        e.L[2].hi = 0;
+        e.L[2].base = 1;
+        dir_at(0) = e;
+        cells[0] = make_int2(wfa_extend<S>(qb, qn, tb, tn, 0, 0), 0);
+    }
+    __syncwarp();
+    if (alive) {
+        used = 1;
+        const int v0 = cells[0].x;
+        // endpoint (wfa_simd.rs:618-650) on frame 0: only diagonal 0 is set
+        if (!fitting) {
+            if (qn - tn == 0 && v0 == qn) {
+                done = true;
+                t_end = tn;
+                k_end = 0;
+                layer_end = 0;
+            }
+        } else if (qn <= tn && v0 == qn) {
+            done = true;
+            t_end = qn;
+            k_end = 0;
+            layer_end = 0;
+        }
+    }
+    int64_t s = 1;
+    for (;;) {
+        const bool run = alive && !done && s <= hard_max_s;
+        if (!__any_sync(PHR_FULL_MASK, run)) break;
+        LayerBand bI = {1, 0, 0}, bD = {1, 0, 0}, bM = {1, 0, 0};
+        LayerBand sMo = {1, 0, 0}, sIe = {1, 0, 0}, sDe = {1, 0, 0}, sMx = {1, 0, 0};
+        if (run) {
+            if (!fits(used, s + 1)) {
+                overflow = true;
+                alive = false;
+            }
+        }
+        bool go = run && alive;
+        if (go) {
+            const int64_t so = s - O - E, se = s - E, sx = s - X;
+            if (so >= 0) sMo = dir_at(so).L[0];
+            if (se >= 0) {
+                sIe = dir_at(se).L[1];
+                sDe = dir_at(se).L[2];
+            }
+            if (sx >= 0) sMx = dir_at(sx).L[0];
+            // I: from M[so] (k-1) and I[se] (k-1): bands shifted by +1
+            int lo = INT32_MAX, hi = INT32_MIN;
+            if (sMo.lo <= sMo.hi) { lo = min(lo, sMo.lo + 1); hi = max(hi, sMo.hi + 1); }
+            if (sIe.lo <= sIe.hi) { lo = min(lo, sIe.lo + 1); hi = max(hi, sIe.hi + 1); }
+            bI.lo = max(lo, -tn);
+            bI.hi = min(hi, qn);
+            // D: from M[so] (k+1) and D[se] (k+1): shifted by -1
+            lo = INT32_MAX;
+            hi = INT32_MIN;
+            if (sMo.lo <= sMo.hi) { lo = min(lo, sMo.lo - 1); hi = max(hi, sMo.hi - 1); }
+            if (sDe.lo <= sDe.hi) { lo = min(lo, sDe.lo - 1); hi = max(hi, sDe.hi - 1); }
+            bD.lo = max(lo, -tn);
+            bD.hi = min(hi, qn);
+            // M: from M[sx] (k), I[s] (k), D[s] (k)
+            lo = INT32_MAX;
+            hi = INT32_MIN;
+            if (sMx.lo <= sMx.hi) { lo = min(lo, sMx.lo); hi = max(hi, sMx.hi); }
+            if (bI.lo <= bI.hi) { lo = min(lo, bI.lo); hi = max(hi, bI.hi); }
+            if (bD.lo <= bD.hi) { lo = min(lo, bD.lo); hi = max(hi, bD.hi); }
+            bM.lo = max(lo, -tn);
+            bM.hi = min(hi, qn);
+            const uint64_t wI = bI.lo <= bI.hi ? static_cast<uint64_t>(bI.hi - bI.lo + 1) : 0;
+            const uint64_t wD = bD.lo <= bD.hi ? static_cast<uint64_t>(bD.hi - bD.lo + 1) : 0;
+            const uint64_t wM = bM.lo <= bM.hi ? static_cast<uint64_t>(bM.hi - bM.lo + 1) : 0;
+            bI.base = used;
+            bD.base = used + wI;
+            bM.base = used + wI + wD;
+            if (!fits(used + wI + wD + wM, s + 1)) {
+                overflow = true;
+                alive = false;
+                go = false;
+            } else {
+                used += wI + wD + wM;
+            }
+        }
+        int best_end_k = INT32_MAX, best_end_layer = 0;
+        if (go && bM.lo <= bM.hi) {
+            // union band == M band (it contains the I and D bands)
+            const int lo = bM.lo, hi = bM.hi;
+            int k = lo + ((gl - ((lo + tn) % G)) % G + G) % G;
+            for (; k <= hi; k += G) {
+                int32_t ins = UNSET, del = UNSET;
+                int32_t iop = 0, dop = 0;
+                if (k >= bI.lo && k <= bI.hi) {
+                    int32_t best = UNSET;
+                    if (k - 1 >= -tn) {
+                        if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
+                            const int32_t pv = cells[sMo.base + (k - 1 - sMo.lo)].x;
+                            if (pv != UNSET) {
+                                const int32_t c = pv + 1;
+                                if (aff_valid(c, k, qn, tn) && c > best) { best = c; iop = 0; }
+                            }
+                        }
+                        if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
+                            const int32_t pv = cells[sIe.base + (k - 1 - sIe.lo)].x;
+                            if (pv != UNSET) {
+                                const int32_t c = pv + 1;
+                                if (aff_valid(c, k, qn, tn) && c > best) { best = c; iop = 1; }
+                            }
+                        }
+                    }
+                    ins = best;
+                    cells[bI.base + (k - bI.lo)] = make_int2(ins, iop);
+                }
+                if (k >= bD.lo && k <= bD.hi) {
+                    int32_t best = UNSET;
+                    if (k + 1 <= qn) {
+                        if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
+                            const int32_t pv = cells[sMo.base + (k + 1 - sMo.lo)].x;
+                            if (pv != UNSET) {
+                                if (aff_valid(pv, k, qn, tn) && pv > best) { best = pv; dop = 0; }
+                            }
+                        }
+                        if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
+                            const int32_t pv = cells[sDe.base + (k + 1 - sDe.lo)].x;
+                            if (pv != UNSET) {
+                                if (aff_valid(pv, k, qn, tn) && pv > best) { best = pv; dop = 1; }
+                            }
+                        }
+                    }
+                    del = best;
+                    cells[bD.base + (k - bD.lo)] = make_int2(del, dop);
+                }
+                // M (wfa_simd.rs:743-765): [mismatch-extend, ins close, del close], strict >
+                int32_t best = UNSET;
+                uint32_t mop = 0;
+                if (k >= sMx.lo && k <= sMx.hi) {
+                    const int32_t pv = cells[sMx.base + (k - sMx.lo)].x;
+                    if (pv != UNSET) {
+                        const int32_t c = pv + 1;
+                        if (aff_valid(c, k, qn, tn) && c > best) { best = c; mop = 0; }
+                    }
+                }
+                if (ins != UNSET && aff_valid(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
+                if (del != UNSET && aff_valid(del, k, qn, tn) && del > best) { best = del; mop = 2; }
+                int32_t mval = UNSET;
+                uint32_t aux = 0;
+                if (best != UNSET) {
+                    mval = wfa_extend<S>(qb, qn, tb, tn, best, k);
+                    aux = (static_cast<uint32_t>(best) << 2) | mop;
+                }
+                cells[bM.base + (k - bM.lo)] = make_int2(mval, static_cast<int32_t>(aux));
+                // endpoint candidates: value == qn in layer order m, ins, del
+                int layer = -1;
+                if (mval == qn) layer = 0;
+                else if (ins == qn) layer = 1;
+                else if (del == qn) layer = 2;
+                if (layer >= 0) {
+                    if (!fitting) {
+                        if (k == qn - tn) { best_end_k = k; best_end_layer = layer; }
+                    } else if (k >= qn - tn && k <= qn && k < best_end_k) {
+                        best_end_k = k;
+                        best_end_layer = layer;
+                    }
+                }
+            }
+        }
+        if (go && gl == 0) {
+            AffDir e;
+            e.L[0] = bM;
+            e.L[1] = bI;
+            e.L[2] = bD;
+            dir_at(s) = e;
+        }
+        // group min over (k, layer): smallest k wins (largest t_end)
+        int kk = best_end_k, ll = best_end_layer;
+        for (int o = 1; o < G; o <<= 1) {
+            const int ok = __shfl_xor_sync(PHR_FULL_MASK, kk, o, G);
+            const int ol = __shfl_xor_sync(PHR_FULL_MASK, ll, o, G);
+            if (ok < kk) { kk = ok; ll = ol; }
+        }
+        __syncwarp();
+        if (go && kk != INT32_MAX) {
+            done = true;
+            s_end = static_cast<int>(s);
+            t_end = qn - kk;
+            k_end = kk;
+            layer_end = ll;
+        }
+        if (run) ++s;
+    }
+    const bool failed = act && !done && !overflow;
+    if (act && overflow && gl == 0) {
+        // retry with 4x the room used so far (bounded by every diagonal of every score)
+        const uint64_t full = runs_bytes + static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
+                              static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull;
+        const uint64_t grow = runs_bytes + 4ull * (used * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) + 4096;
+        report_redo(P, pid, min(full, grow));
+    }
+
+    // ---- traceback (wfa_simd.rs:785-886) ----
+    RunWriter rw;
+    rw.init(runs, static_cast<uint32_t>(qn + tn + 2));
+    const bool trace = act && done;
+    uint32_t n_edit = 0;
+    if (trace && gl == 0) {
+        int qi = qn, ti = t_end, k = k_end, ss = s_end, layer = layer_end;
+        int guard = 4 * (qn + tn) + 16;
+        while ((qi > 0 || ti > 0) && guard-- > 0) {
+            if (ss == 0) {
+                const int mm = min(qi, ti);
+                rw.push(0, static_cast<uint32_t>(mm));
+                qi -= mm;
+                ti -= mm;
+                break;
+            }
+            const AffDir e = dir_at(ss);
+            if (layer == 0) {
+                const int2 c = cells[e.L[0].base + (k - e.L[0].lo)];
+                const uint32_t aux = static_cast<uint32_t>(c.y);
+                const uint32_t mop = aux & 3;
+                const int32_t raw = static_cast<int32_t>(aux >> 2);
+                const int mc = max(qi - raw, 0);
+                if (mc > 0) {
+                    rw.push(0, static_cast<uint32_t>(mc));
+                    qi -= mc;
+                    ti -= mc;
+                }
+                if (mop == 0) {
+                    rw.push(1, 1);
+                    --qi;
+                    --ti;
+                    ++n_edit;
+                    ss -= X;
+                } else {
+                    layer = static_cast<int>(mop);
+                }
+            } else if (layer == 1) {
+                rw.push(3, 1);  // ins (query-extra) -> 'D'
+                --qi;
+                ++n_edit;
+                const int2 c = cells[e.L[1].base + (k - e.L[1].lo)];
+                if (c.y == 0) {
+                    ss -= O + E;
+                    layer = 0;
+                } else {
+                    ss -= E;
+                }
+                k -= 1;
+            } else {
+                rw.push(2, 1);  // del (target-extra) -> 'I'
+                --ti;
+                ++n_edit;
+                const int2 c = cells[e.L[2].base + (k - e.L[2].lo)];
+                if (c.y == 0) {
+                    ss -= O + E;
+                    layer = 0;
+                } else {
+                    ss -= E;
+                }
+                k += 1;
+            }
+        }
+        if (guard < 0) atomicOr(P.error_flag, 4u);
+        rw.flush();
+    }
+    const int leader = lane_id() & ~(G - 1);
+    const uint32_t nr = __shfl_sync(PHR_FULL_MASK, rw.n, leader);
+    const bool ovf = __shfl_sync(PHR_FULL_MASK, rw.overflow ? 1 : 0, leader) != 0;
+    const uint32_t ned = __shfl_sync(PHR_FULL_MASK, n_edit, leader);
+    __syncwarp();
+    const uint32_t nr_fmt = (trace && !ovf) ? nr : 0;
+    char* out = act ? P.text + P.text_off[pid] : nullptr;
+    const uint32_t tl = format_group(runs, nr_fmt, out, G);
+    if (act && gl == 0) {
+        if (trace && !ovf) {
+            PairOut o;
+            o.status = PHR_OK;
+            o.ed = static_cast<int32_t>(ned);  // levenshtein_from_cigar: X + I/D lengths
+            o.t_consumed = t_end;
+            o.affine_score = s_end;
+            o.n_runs = nr;
+            o.text_len = tl;
+            P.out[pid] = o;
+        } else if (failed) {
+            PairOut o = {};
+            o.status = PHR_ALIGNMENT_FAILED;
+            P.out[pid] = o;
+        } else if (trace && ovf) {
+            atomicOr(P.error_flag, 2u);
+        }
+    }
+}
+
+// Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
+template <class S, bool kAffine>
+__global__ void __launch_bounds__(256) wfa_kernel(ExtendParams P) {
+    const int lane = lane_id();
+    const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    uint8_t* slot = P.scratch + warp_global * P.slot_bytes;
+    for (;;) {
+        uint32_t task = 0;
+        if (lane == 0) task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
+        task = __shfl_sync(PHR_FULL_MASK, task, 0);
+        if (task >= P.tasks.range[1]) break;
+        const int G = P.tasks.task_group[task];
+        const int count = P.tasks.task_count[task];
+        const int grp = lane / G;
+        bool act = grp < count;
+        const uint32_t pid = act ? P.tasks.order[P.tasks.task_first[task] + grp] : 0;
+        PairDesc d = {};
+        if (act) d = P.desc[pid];
+        // pairs of the other symbol mode run in the other instantiation
+        act = act && d.mode == (S::kBits == 2 ? 0 : 1);
+        if (!__any_sync(PHR_FULL_MASK, act)) continue;
+        const uint64_t region_bytes = (P.slot_bytes / (32 / G)) & ~15ull;
+        uint8_t* region = slot + static_cast<uint64_t>(grp) * region_bytes;
+        if (kAffine)
+            wfa_affine_group<S>(P, d, pid, act, G, region, region_bytes);
+        else
+            wfa_linear_group<S>(P, d, pid, act, G, region, region_bytes);
+    }
+}
+
+}  // namespace
+
+void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st) {
+    wfa_kernel<Seq2, false><<<grid, block, 0, st>>>(p);
+}
+void launch_wfa_linear_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st) {
+    wfa_kernel<SeqB, false><<<grid, block, 0, st>>>(p);
+}
+void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st) {
+    wfa_kernel<Seq2, true><<<grid, block, 0, st>>>(p);
+}
+void launch_wfa_affine_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st) {
+    wfa_kernel<SeqB, true><<<grid, block, 0, st>>>(p);
+}
+
+}  // namespace phr

@@ -1,0 +1,152 @@
+"""GPU parity of the extension engines (WFA linear/affine, Myers fitting/global)
+against the CPU oracle, through the C ABI. Bit-exact: status, CIGAR, edit distance
+and all four coordinates must be identical."""
+import numpy as np
+import pytest
+
+import known
+import oracle as O
+import refgen as R
+from phraya_b200 import _abi as A
+from phraya_b200 import api as P
+from phraya_b200 import datagen as D
+
+pytestmark = pytest.mark.gpu
+ENGINES = [A.ENGINE_WFA_LINEAR, A.ENGINE_WFA_AFFINE, A.ENGINE_MYERS_FIT, A.ENGINE_MYERS_GLOBAL]
+NAMES = {0: "wfa", 1: "affine", 2: "myers_fit", 3: "myers_global"}
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = P.Engine(0)
+    yield e
+    e.close()
+
+
+def gpu_align(eng):
+    def f(engine, q, t, qseed, tseed):
+        return eng.extend(engine, [(q, t, qseed, tseed)])[0]
+    return f
+
+
+def compare(eng, engine, pairs, costs=(2, 4, 1)):
+    packed = pairs if isinstance(pairs, O.PackedPairs) else O.PackedPairs(pairs)
+    ga, gc = eng.extend_packed(engine, packed, P.AffineCosts(*costs))
+    oa, oc = O.extend_packed(engine, packed, costs)
+    g = P.unpack(ga, gc)
+    o = P.unpack(oa, oc)
+    bad = [i for i in range(packed.n) if g[i] != o[i]]
+    if bad:
+        i = bad[0]
+        q = bytes(packed.seq[packed.q_off[i]:packed.q_off[i] + packed.q_len[i]])
+        t = bytes(packed.seq[packed.t_off[i]:packed.t_off[i] + packed.t_len[i]])
+        raise AssertionError(f"{NAMES[engine]}: {len(bad)}/{packed.n} differ; first #{i}\n gpu={g[i]}\n "
+                             f"ref={o[i]}\n q={q[:400]!r}\n t={t[:400]!r}")
+    if engine == A.ENGINE_WFA_AFFINE:
+        assert np.array_equal(ga["affine_score"], oa["affine_score"])
+    return g
+
+
+KA = known.load()
+
+
+@pytest.mark.parametrize("case", KA["cases"], ids=[c["src"] for c in KA["cases"]])
+def test_known_answer_gpu(eng, case):
+    known.check_case(case, gpu_align(eng))
+
+
+@pytest.mark.parametrize("case", KA["pairs_equal"], ids=[c["src"] for c in KA["pairs_equal"]])
+def test_engines_agree_gpu(eng, case):
+    known.check_pair(case, gpu_align(eng))
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=[NAMES[e] for e in ENGINES])
+def test_reference_sweeps_bit_exact(eng, engine):
+    cases = (R.scalar_edit_sweep() + R.affine_fitting_cases() + R.affine_global_cases() +
+             R.myers_wfa_fitting_sweep())
+    compare(eng, engine, cases)
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=[NAMES[e] for e in ENGINES])
+def test_microbench_pairs_bit_exact(eng, engine):
+    packed = D.extension_pairs(3000, 100, 300, 0.05, seed=11)
+    compare(eng, engine, packed)
+    if engine == A.ENGINE_WFA_AFFINE:
+        compare(eng, engine, packed, costs=(4, 6, 2))
+
+
+def test_myers_long_pairs_bit_exact(eng):
+    packed = D.extension_pairs(300, 64, 2048, 0.05, seed=12, log_uniform=True)
+    compare(eng, A.ENGINE_MYERS_GLOBAL, packed)
+    compare(eng, A.ENGINE_MYERS_FIT, packed)
+
+
+def test_fitting_windows_and_seeds(eng):
+    # read vs 2x window (fitting branch), anchors at nonzero offsets
+    rng = np.random.default_rng(5)
+    pairs = []
+    for i in range(600):
+        t = bytes(rng.choice(list(b"ACGT"), 700).tolist())
+        ql = int(rng.integers(50, 300))
+        s = int(rng.integers(0, 200))
+        q = bytearray(t[s:s + ql])
+        for _ in range(int(rng.integers(0, 6))):
+            q[int(rng.integers(0, len(q)))] = int(rng.choice(list(b"ACGT")))
+        pairs.append((bytes(q), t, 0, s if i % 3 else max(0, s - 3)))
+    for e in ENGINES:
+        compare(eng, e, pairs)
+
+
+def test_high_divergence_and_unrelated(eng):
+    # large scores exercise the overflow redo passes
+    rng = np.random.default_rng(6)
+    pairs = []
+    for _ in range(120):
+        ql, tl = int(rng.integers(20, 400)), int(rng.integers(20, 800))
+        pairs.append((bytes(rng.choice(list(b"ACGT"), ql).tolist()), bytes(rng.choice(list(b"ACGT"), tl).tolist())))
+    for e in ENGINES:
+        compare(eng, e, pairs)
+
+
+def test_multi_stripe_myers(eng):
+    packed = D.extension_pairs(12, 2100, 4200, 0.03, seed=13)
+    compare(eng, A.ENGINE_MYERS_GLOBAL, packed)
+    compare(eng, A.ENGINE_MYERS_FIT, packed)
+
+
+def test_byte_path_non_acgt(eng):
+    # lowercase, N and protein letters take the byte path; comparisons stay exact bytes
+    rng = np.random.default_rng(7)
+    pairs = []
+    alph = list(b"ACDEFGHIKLMNPQRSTVWY")
+    for i in range(300):
+        L = int(rng.integers(5, 500))
+        q = bytearray(rng.choice(alph if i % 2 else list(b"ACGTN"), L).tolist())
+        t = bytearray(q)
+        for _ in range(int(rng.integers(0, 20))):
+            p = int(rng.integers(0, len(t)))
+            t[p] = int(rng.choice(alph))
+        if i % 5 == 0:
+            t = t.lower()
+        if i % 7 == 0:
+            t = t + bytes(rng.choice(alph, 300).tolist())
+        pairs.append((bytes(q), bytes(t)))
+    for e in ENGINES:
+        compare(eng, e, pairs)
+
+
+def test_edges(eng):
+    pairs = [(b"", b""), (b"", b"ACGT"), (b"ACG", b""), (b"A", b"A"), (b"A", b"C"), (b"ACGT", b"ACGT", 4, 4),
+             (b"ACGT", b"ACGT", 5, 0), (b"ACGT", b"ACGT", 0, 5), (b"ACGTACGT", b"ACGT", 8, 0), (b"N", b"N"),
+             (b"ACGT" * 40, b"")]
+    for e in ENGINES:
+        compare(eng, e, pairs)
+        compare(eng, e, pairs, costs=(4, 6, 2))
+
+
+def test_percall_matches_batched(eng):
+    packed = D.extension_pairs(40, 100, 300, 0.05, seed=14)
+    for e in ENGINES:
+        a1, c1 = eng.extend_packed(e, packed)
+        a2, c2 = eng.extend_packed(e, packed, percall=True)
+        assert P.unpack(a1, c1) == P.unpack(a2, c2)
