@@ -1,0 +1,366 @@
+"""Benchmark: phraya-align's batched extension microbench on B200.
+
+Workload (one step = the whole job, all pairs resident in HBM):
+  set A: N_A query/target pairs, query lengths uniform in [100, 300] bp, targets =
+         query mutated at per-pair divergence U[0, 5 %] (70 % substitutions, 30 % 1-5 bp
+         indels); aligned with WFA affine (mismatch 4, gap open 6, gap extend 2) AND WFA
+         linear;
+  set B: N_B pairs with lengths log-uniform in [64, 2048] bp, same mutation model;
+         aligned with Myers bit-parallel edit distance + CIGAR (myers_edit_distance).
+Metric: aligned pairs per second over the whole job (2 N_A + N_B alignments per step);
+DP-equivalent GCUPS (sum q*t / s) is reported beside it. Synthetic seeded data.
+
+Run: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "reads/s & GCUPS on 1 B200, served vs per-call GPU; p50/p99 latency; bit-exact"
+N_A_DEFAULT = 1_000_000
+N_B_DEFAULT = 1_000_000
+COSTS_A = (4, 6, 2)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device=0):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxs, reasons = [], [], set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxs.append(float(parts[2]))
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxs) if maxs else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def make_workload(n_a, n_b, seed):
+    from phraya_b200 import datagen as D
+    set_a = D.extension_pairs(n_a, 100, 300, 0.05, seed=seed)
+    set_b = D.extension_pairs(n_b, 64, 2048, 0.05, seed=seed + 1000, log_uniform=True)
+    return set_a, set_b
+
+
+def dp_cells(p):
+    return float(np.dot(p.q_len.astype(np.float64), p.t_len.astype(np.float64)))
+
+
+def input_bytes(p):
+    return int(p.seq.nbytes + p.q_off.nbytes + p.q_len.nbytes + p.t_off.nbytes + p.t_len.nbytes)
+
+
+def cpu_baseline(set_a, set_b, n_a, n_b, nthreads, sample_a=60000, sample_b=6000):
+    """Times the oracle (CPU restatement) on a bounded sample and scales to the job."""
+    import oracle as O
+    from phraya_b200 import _abi as A
+    from phraya_b200.batch import PackedPairs
+
+    def sub(p, k):
+        k = min(k, p.n)
+        return PackedPairs.from_arrays(p.seq, p.q_off[:k].copy(), p.q_len[:k].copy(), p.t_off[:k].copy(),
+                                       p.t_len[:k].copy())
+
+    sa, sb = sub(set_a, sample_a), sub(set_b, sample_b)
+    L = O.lib()
+    t = {}
+    for name, eng, p, costs in (("affine", A.ENGINE_WFA_AFFINE, sa, COSTS_A), ("linear", A.ENGINE_WFA_LINEAR, sa, (2, 4, 1)),
+                                ("myers", A.ENGINE_MYERS_GLOBAL, sb, (2, 4, 1))):
+        b = p.batch()
+        t0 = time.perf_counter()
+        L.orc_extend_batch_time(eng, b, A.AffineCosts(*costs), nthreads)
+        t[name] = time.perf_counter() - t0
+    job_s = (t["affine"] + t["linear"]) * (n_a / sa.n) + t["myers"] * (n_b / sb.n)
+    return {"value": (2 * n_a + n_b) / job_s, "unit": "pairs/s", "cores": nthreads, "kind": "port",
+            "sample": f"{sa.n} set-A pairs (WFA affine 4/6/2 + WFA linear) and {sb.n} set-B pairs (Myers), "
+                      f"scaled to {n_a}+{n_a}+{n_b} alignments; {t['affine']:.2f}+{t['linear']:.2f}+{t['myers']:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's CPU algorithm (the oracle restatement; the Rust
+    reference cannot be built without a Rust toolchain) on the host cores."""
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    n_a, n_b = args.n_a, args.n_b
+    set_a, set_b = make_workload(min(n_a, 60000), min(n_b, 6000), seed=0)
+    vals = []
+    base = None
+    for s in range(args.warmup + args.steps):
+        base = cpu_baseline(set_a, set_b, n_a, n_b, nthreads, sample_a=set_a.n, sample_b=set_b.n)
+        if s >= args.warmup:
+            vals.append(base["value"])
+    v = statistics.median(vals)
+    ms = (2 * n_a + n_b) / v * 1000.0
+    line = {"metric": METRIC, "value": v, "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+            "config": {"workload": "batched extension microbench", "n_pairs_wfa": n_a, "n_pairs_myers": n_b,
+                       "note": "CPU restatement of phraya-align (Rust toolchain absent); bounded sample per step"},
+            "cpu_baseline": {**base, "value": v},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_engine(args, rank, world):
+    import ctypes as C
+
+    import torch
+
+    from phraya_b200 import _abi as A
+    from phraya_b200 import api as P
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    n_a, n_b = args.n_a, args.n_b
+    t_gen = time.perf_counter()
+    set_a, set_b = make_workload(n_a, n_b, seed=rank)
+    t_gen = time.perf_counter() - t_gen
+    eng = P.Engine(dev)
+    L = eng._lib
+    stream = torch.cuda.ExternalStream(L.phr_ctx_stream(eng.handle), device=dev)
+
+    # ---- device-resident copies (value) --------------------------------------
+    def to_dev(p):
+        d = {k: torch.from_numpy(np.ascontiguousarray(getattr(p, k))).to(f"cuda:{dev}")
+             for k in ("seq", "q_off", "q_len", "t_off", "t_len")}
+        b = A.PairBatch()
+        b.n_pairs = p.n
+        b.seq = d["seq"].data_ptr()
+        b.seq_bytes = p.seq.nbytes
+        b.q_off, b.q_len = d["q_off"].data_ptr(), d["q_len"].data_ptr()
+        b.t_off, b.t_len = d["t_off"].data_ptr(), d["t_len"].data_ptr()
+        b.q_seed = b.t_seed = None
+        cap = int(0.75 * (p.q_len.sum() + p.t_len.sum())) + 64 * p.n
+        aln = torch.empty(p.n * C.sizeof(A.Alignment), dtype=torch.uint8, device=f"cuda:{dev}")
+        cig = torch.empty(cap, dtype=torch.uint8, device=f"cuda:{dev}")
+        arena = A.ResultArena(aln.data_ptr(), cig.data_ptr(), cap, 0)
+        return d, b, aln, cig, arena
+
+    jobs = [(A.ENGINE_WFA_AFFINE, COSTS_A, *to_dev(set_a)), (A.ENGINE_WFA_LINEAR, (2, 4, 1), *to_dev(set_a)),
+            (A.ENGINE_MYERS_GLOBAL, (2, 4, 1), *to_dev(set_b))]
+    torch.cuda.synchronize()
+
+    def step():
+        for eng_id, costs, _d, b, _aln, _cig, arena in jobs:
+            eng.check(L.phr_extend_batch_device(eng.handle, eng_id, C.byref(b), A.AffineCosts(*costs),
+                                                C.byref(arena)))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    L.phr_ctx_reset_timing(eng.handle)
+    L.phr_ctx_set_timing(eng.handle, 1)
+    launches0 = eng.kernel_launches
+    clocks = ClockSampler(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    L.phr_ctx_set_timing(eng.handle, 0)
+    launches = eng.kernel_launches - launches0
+    elapsed_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    per_step_pairs = 2 * n_a + n_b
+    value = per_step_pairs * world / (ms_per_step / 1000.0)
+    cells = 2 * dp_cells(set_a) + dp_cells(set_b)
+    gcups = cells * world / (ms_per_step / 1000.0) / 1e9
+
+    # per-kernel device times (CUDA events on the launching stream)
+    recs = (A.KernelTiming * 64)()
+    nrec = L.phr_ctx_get_timing(eng.handle, recs, 64)
+    ktimes = {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(min(nrec, 64))}
+
+    # ---- end to end through the host API, pinned host buffers ----------------
+    def pinned_pairs(p):
+        from phraya_b200.batch import PackedPairs
+        arrs = {}
+        for k in ("seq", "q_off", "q_len", "t_off", "t_len"):
+            src = np.ascontiguousarray(getattr(p, k))
+            t = torch.empty(src.shape, dtype=torch.from_numpy(src[:1]).dtype, pin_memory=True)
+            t.numpy()[...] = src
+            arrs[k] = t
+        pp = PackedPairs.from_arrays(*(arrs[k].numpy() for k in ("seq", "q_off", "q_len", "t_off", "t_len")))
+        pp._pins = arrs
+        return pp
+
+    pa, pb = pinned_pairs(set_a), pinned_pairs(set_b)
+
+    def host_outputs(p):
+        aln = torch.empty(p.n * C.sizeof(A.Alignment), dtype=torch.uint8, pin_memory=True)
+        cap = int(0.75 * (p.q_len.sum() + p.t_len.sum())) + 64 * p.n
+        cig = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+        return aln, cig, cap
+
+    outs = [host_outputs(pa), host_outputs(pa), host_outputs(pb)]
+    e2e_jobs = [(A.ENGINE_WFA_AFFINE, COSTS_A, pa, outs[0]), (A.ENGINE_WFA_LINEAR, (2, 4, 1), pa, outs[1]),
+                (A.ENGINE_MYERS_GLOBAL, (2, 4, 1), pb, outs[2])]
+    d2h = 0
+
+    def e2e_step():
+        nonlocal d2h
+        d2h = 0
+        for eng_id, costs, p, (aln, cig, cap) in e2e_jobs:
+            arena = A.ResultArena(aln.data_ptr(), cig.data_ptr(), cap, 0)
+            b = p.batch()
+            eng.check(L.phr_extend_batch(eng.handle, eng_id, C.byref(b), A.AffineCosts(*costs), C.byref(arena)))
+            d2h += p.n * C.sizeof(A.Alignment) + arena.cigar_used
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = 2 * input_bytes(set_a) + input_bytes(set_b)
+
+    if rank != 0:
+        return
+    # ---- roofline of the dominant kernel --------------------------------------
+    peaks, peak_src = load_peaks()
+    name, (nl, tot) = max(ktimes.items(), key=lambda kv: kv[1][1])
+    per_launch_ms = tot / nl
+    sm_clock = (clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0))
+    int_peak_tops = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    if name.startswith("myers"):
+        ops = dp_cells(set_b) * 22.0 / 32.0      # per launch: one Myers pass over set B
+        achieved = ops / (per_launch_ms / 1000.0) / 1e12
+        roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tops/s",
+                "frac": achieved / int_peak_tops, "traffic": None, "kernel": name,
+                "work": "sum(m*n) * 22/32 integer ops per launch (set B)",
+                "peak_source": "nominal issue rate 148 SMs x 4 x 32 lanes x max SM clock (no measured int peak)"}
+    else:
+        # WFA: DP-equivalent cells of set A per launch against the same issue peak
+        ops = dp_cells(set_a)
+        achieved = ops / (per_launch_ms / 1000.0) / 1e12
+        roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tcells/s",
+                "frac": achieved / int_peak_tops, "traffic": None, "kernel": name,
+                "work": "DP-equivalent cells of set A per launch",
+                "peak_source": "nominal issue rate (no measured int peak)"}
+    cpu = cpu_baseline(set_a, set_b, n_a, n_b, os.cpu_count() or 1) if not args.no_cpu else None
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
+            "config": {"workload": "batched extension microbench", "n_pairs_wfa": n_a, "n_pairs_myers": n_b,
+                       "wfa_affine_costs": list(COSTS_A), "lengths_wfa": [100, 300],
+                       "lengths_myers": [64, 2048, "log-uniform"], "divergence": [0.0, 0.05],
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "gcups_dp_equivalent": gcups,
+            "e2e": {"value": per_step_pairs * world / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1000.0},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "kernel_ms": {k: round(v[1] / args.steps, 3) for k, v in ktimes.items()},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+            "datagen_s": round(t_gen, 1)}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n-a", type=int, default=N_A_DEFAULT)
+    ap.add_argument("--n-b", type=int, default=N_B_DEFAULT)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "engine":
+        import datetime
+
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_engine(args, rank, world)
+    finally:
+        if world > 1 and args.impl == "engine":
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

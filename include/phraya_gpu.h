@@ -125,6 +125,24 @@ const char* phr_ctx_last_error(const phr_ctx* ctx);
 /* Number of the library's own kernel launches issued on this context so far. */
 uint64_t phr_ctx_kernel_launches(const phr_ctx* ctx);
 
+/*
+ * Instrumentation (no counterpart in the reference). With timing enabled, every
+ * kernel the library launches is bracketed by CUDA events on the context's stream and
+ * its device time accumulated per kernel name.
+ */
+typedef struct {
+    char name[32];
+    uint64_t launches;
+    double total_ms;
+} phr_kernel_timing;
+
+phr_status phr_ctx_set_timing(phr_ctx* ctx, int32_t enable);
+/* Copies up to `max` per-kernel records; returns how many kernels have records. */
+uint32_t phr_ctx_get_timing(const phr_ctx* ctx, phr_kernel_timing* out, uint32_t max);
+void phr_ctx_reset_timing(phr_ctx* ctx);
+/* The cudaStream_t the context launches on (for callers that order their own work). */
+void* phr_ctx_stream(const phr_ctx* ctx);
+
 /* ------------------------------------------------------------------------- */
 /* Pairs API -- replaces per-call wfa_extend / wfa_extend_affine /            */
 /* myers_extend / myers_edit_distance (phraya-align/src/lib.rs:63-167).       */

@@ -222,6 +222,10 @@ class ServerResult(C.Structure):
     ]
 
 
+class KernelTiming(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_uint64), ("total_ms", C.c_double)]
+
+
 # Every exported symbol of libphraya_b200.so, with its ctypes prototype.
 PROTOTYPES = {
     "phr_abi_version": (C.c_int32, []),
@@ -230,6 +234,10 @@ PROTOTYPES = {
     "phr_ctx_destroy": (None, [C.c_void_p]),
     "phr_ctx_last_error": (C.c_char_p, [C.c_void_p]),
     "phr_ctx_kernel_launches": (C.c_uint64, [C.c_void_p]),
+    "phr_ctx_set_timing": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "phr_ctx_get_timing": (C.c_uint32, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "phr_ctx_reset_timing": (None, [C.c_void_p]),
+    "phr_ctx_stream": (C.c_void_p, [C.c_void_p]),
     "phr_extend_batch": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(PairBatch), AffineCosts,
                                      C.POINTER(ResultArena)]),
     "phr_extend_batch_device": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(PairBatch), AffineCosts,

@@ -152,6 +152,36 @@ void phr_ctx_destroy(phr_ctx* c) {
     delete c;
 }
 
+phr_status phr_ctx_set_timing(phr_ctx* c, int32_t enable) {
+    if (!c) return PHR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->impl.mu);
+    c->impl.timing = enable != 0;
+    return PHR_OK;
+}
+
+uint32_t phr_ctx_get_timing(const phr_ctx* c, phr_kernel_timing* out, uint32_t max) {
+    if (!c) return 0;
+    uint32_t i = 0;
+    for (const auto& kv : c->impl.timings) {
+        if (out && i < max) {
+            std::memset(&out[i], 0, sizeof(out[i]));
+            std::strncpy(out[i].name, kv.first.c_str(), sizeof(out[i].name) - 1);
+            out[i].launches = kv.second.first;
+            out[i].total_ms = kv.second.second;
+        }
+        ++i;
+    }
+    return i;
+}
+
+void phr_ctx_reset_timing(phr_ctx* c) {
+    if (!c) return;
+    std::lock_guard<std::mutex> lk(c->impl.mu);
+    c->impl.timings.clear();
+}
+
+void* phr_ctx_stream(const phr_ctx* c) { return c ? static_cast<void*>(c->impl.stream) : nullptr; }
+
 const char* phr_ctx_last_error(const phr_ctx* c) { return c ? c->impl.last_error.c_str() : "null context"; }
 
 uint64_t phr_ctx_kernel_launches(const phr_ctx* c) { return c ? c->impl.launches.load() : 0; }

@@ -47,7 +47,43 @@ DeviceArena::~DeviceArena() {
     if (base) cudaFree(base);
 }
 
+void Ctx::begin_kernel(const char* name, cudaEvent_t* a) {
+    if (cudaEventCreate(a) != cudaSuccess) {
+        *a = nullptr;
+        return;
+    }
+    cudaEventRecord(*a, stream);
+}
+
+void Ctx::end_kernel(const char* name, cudaEvent_t a) {
+    cudaEvent_t b;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return;
+    }
+    cudaEventRecord(b, stream);
+    pending.push_back({name, a, b});
+}
+
+void Ctx::resolve_timings() {
+    for (auto& p : pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            auto& t = timings[p.name];
+            t.first += 1;
+            t.second += ms;
+        }
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    pending.clear();
+}
+
 Ctx::~Ctx() {
+    for (auto& p : pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
     if (d_counters) cudaFree(d_counters);
     if (h_pinned) cudaFreeHost(h_pinned);
     if (stream) cudaStreamDestroy(stream);
@@ -521,8 +557,10 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
 
     const unsigned T = 256;
     PrepParams pp{in, engine, costs, desc, pout, w2, wb, tb};
-    prep_sizes_kernel<<<blocks_for(n, T), T, 0, st>>>(pp);
-    ++ctx->launches;
+    {
+        KernelScope ks(ctx, "prep_sizes");
+        prep_sizes_kernel<<<blocks_for(n, T), T, 0, st>>>(pp);
+    }
     size_t tn_ = t_need;
     cub::DeviceScan::ExclusiveSum(tmp, tn_, w2, w2o, static_cast<int>(n), st);
     tn_ = t_need;
@@ -532,23 +570,36 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
 
     PackParams pk{in, engine, costs, desc, pout, w2o, wbo, tbo, arena2, arenab, text, keys, vals,
                   ctx->tune.wfa_group_short, ctx->tune.wfa_group_long};
-    pack_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(pk);
-    ++ctx->launches;
+    {
+        KernelScope ks(ctx, "pack");
+        pack_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(pk);
+    }
     tn_ = t_need;
     cub::DeviceRadixSort::SortPairs(tmp, tn_, keys, keys_s, vals, order, static_cast<int>(n), 0, 32, st);
 
     TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, desc,
                   engine, ctx->tune.myers_band_base, need_max};
-    task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    {
+        KernelScope ks(ctx, "task_head");
+        task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    }
     tn_ = t_need;
     cub::DeviceScan::InclusiveScan(tmp, tn_, head, head_s, cub::Max(), static_cast<int>(n), st);
     tbp.head = head_s;
-    task_flag_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    {
+        KernelScope ks(ctx, "task_flag");
+        task_flag_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    }
     tn_ = t_need;
     cub::DeviceScan::ExclusiveSum(tmp, tn_, flag, tidx, static_cast<int>(n), st);
-    task_fill_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
-    task_finalize_kernel<<<1, 1, 0, st>>>(tbp);
-    ctx->launches += 4;
+    {
+        KernelScope ks(ctx, "task_fill");
+        task_fill_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
+    }
+    {
+        KernelScope ks(ctx, "task_finalize");
+        task_finalize_kernel<<<1, 1, 0, st>>>(tbp);
+    }
 
     // slot size for the main pass
     uint64_t h_need = 0;
@@ -591,23 +642,31 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         P.tasks.task_count = tcount;
         P.tasks.task_group = tgroup;
         PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 5, 0, 8, st));
+        const char* kname = is_myers ? "myers" : engine == PHR_ENGINE_WFA_LINEAR ? "wfa_linear" : "wfa_affine";
+        const char* kname_b = is_myers ? "myers_bytes" : engine == PHR_ENGINE_WFA_LINEAR ? "wfa_linear_bytes"
+                                                                                       : "wfa_affine_bytes";
         P.tasks.range = range0;
         P.queue_head = cnt + 5;
-        if (is_myers)
-            launch_myers(P, static_cast<int>(grid), block, st);
-        else if (engine == PHR_ENGINE_WFA_LINEAR)
-            launch_wfa_linear(P, static_cast<int>(grid), block, st);
-        else
-            launch_wfa_affine(P, static_cast<int>(grid), block, st);
+        {
+            KernelScope ks(ctx, kname);
+            if (is_myers)
+                launch_myers(P, static_cast<int>(grid), block, st);
+            else if (engine == PHR_ENGINE_WFA_LINEAR)
+                launch_wfa_linear(P, static_cast<int>(grid), block, st);
+            else
+                launch_wfa_affine(P, static_cast<int>(grid), block, st);
+        }
         P.tasks.range = range1;
         P.queue_head = cnt + 6;
-        if (is_myers)
-            launch_myers_bytes(P, static_cast<int>(grid), block, st);
-        else if (engine == PHR_ENGINE_WFA_LINEAR)
-            launch_wfa_linear_bytes(P, static_cast<int>(grid), block, st);
-        else
-            launch_wfa_affine_bytes(P, static_cast<int>(grid), block, st);
-        ctx->launches += 2;
+        {
+            KernelScope ks(ctx, kname_b);
+            if (is_myers)
+                launch_myers_bytes(P, static_cast<int>(grid), block, st);
+            else if (engine == PHR_ENGINE_WFA_LINEAR)
+                launch_wfa_linear_bytes(P, static_cast<int>(grid), block, st);
+            else
+                launch_wfa_affine_bytes(P, static_cast<int>(grid), block, st);
+        }
         PHR_CUDA_TRY(ctx, cudaGetLastError());
         return PHR_OK;
     };
@@ -630,10 +689,13 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         if (h_need2 > ctx->scratch_budget)
             return set_error(ctx, PHR_ERR_OOM, "a single pair needs more scratch than the workspace budget");
         // tasks from the redo list; swap lists so the pass can append fresh overflows
-        redo_tasks_kernel<<<blocks_for(h_redo[0], T), T, 0, st>>>(rlist, cnt + 7, desc, engine,
-                                                                 ctx->tune.wfa_group_short, ctx->tune.wfa_group_long,
-                                                                 task_first, task_count, task_group, cnt + 14);
-        ++ctx->launches;
+        {
+            KernelScope ks(ctx, "redo_tasks");
+            redo_tasks_kernel<<<blocks_for(h_redo[0], T), T, 0, st>>>(rlist, cnt + 7, desc, engine,
+                                                                     ctx->tune.wfa_group_short,
+                                                                     ctx->tune.wfa_group_long, task_first,
+                                                                     task_count, task_group, cnt + 14);
+        }
         // byte-mode and 2-bit pairs share this list: both launches walk all of it
         PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cnt + 16, cnt + 14, 8, cudaMemcpyDeviceToDevice, st));
         PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 7, 0, 4, st));
@@ -644,22 +706,31 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     }
 
     // pack CIGAR text
-    text_len_kernel<<<blocks_for(n, T), T, 0, st>>>(pout, n, tlen);
+    {
+        KernelScope ks(ctx, "text_len");
+        text_len_kernel<<<blocks_for(n, T), T, 0, st>>>(pout, n, tlen);
+    }
     tn_ = t_need;
     cub::DeviceScan::ExclusiveSum(tmp, tn_, tlen, cigoff, static_cast<int>(n), st);
-    total_kernel<<<1, 1, 0, st>>>(cigoff, tlen, n, total);
+    {
+        KernelScope ks(ctx, "total");
+        total_kernel<<<1, 1, 0, st>>>(cigoff, tlen, n, total);
+    }
     uint64_t h_total = 0;
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_total, total, 8, cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (h_total > res->cigar_capacity)
         return set_error(ctx, PHR_ERR_CAPACITY, "CIGAR arena too small: need " + std::to_string(h_total) + " bytes");
     FinishParams F{n, engine, desc, pout, tbo, text, cigoff, res->aln, res->cigar, res->cigar_capacity, cnt + 10};
-    finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
-    ctx->launches += 3;
+    {
+        KernelScope ks(ctx, "finish");
+        finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
+    }
     uint32_t h_err = 0;
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_err, cnt + 10, 4, cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     PHR_CUDA_TRY(ctx, cudaGetLastError());
+    if (ctx->timing) ctx->resolve_timings();
     if (h_err) return set_error(ctx, PHR_ERR_CUDA, "internal consistency check failed (flags " + std::to_string(h_err) + ")");
     res->cigar_used = h_total;
     return PHR_OK;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -49,7 +50,32 @@ struct Ctx {
     std::mutex mu;
     uint32_t* d_counters = nullptr;   // small device scratch for counters (pinned size)
     void* h_pinned = nullptr;         // small pinned host buffer for D2H of counters
+    // kernel timing (phr_ctx_set_timing)
+    bool timing = false;
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::map<std::string, std::pair<uint64_t, double>> timings;
+    void begin_kernel(const char* name, cudaEvent_t* a);
+    void end_kernel(const char* name, cudaEvent_t a);
+    void resolve_timings();   // after a stream sync
     ~Ctx();
+};
+
+// Brackets one kernel launch with timing events when enabled and counts it.
+struct KernelScope {
+    Ctx* ctx;
+    const char* name;
+    cudaEvent_t a = nullptr;
+    KernelScope(Ctx* c, const char* n) : ctx(c), name(n) {
+        ++ctx->launches;
+        if (ctx->timing) ctx->begin_kernel(name, &a);
+    }
+    ~KernelScope() {
+        if (ctx->timing && a) ctx->end_kernel(name, a);
+    }
 };
 
 // Device-resident description of a pair batch (pointers into device memory).
