@@ -1172,10 +1172,12 @@ void align_read(const Target& tg, const uint8_t* read, size_t len, const phr_ali
     if (!fchains.empty() && rchains.empty()) {
         fok = extend_chains(tg, cfg, read, len, fchains, &fsc);
     } else if (fchains.empty() && !rchains.empty()) {
-        rok = extend_chains(tg, cfg, rc.data(), len, rchains, &rsc);
+        rok = extend_chains(tg, cfg, rc.data(), rc.size(), rchains, &rsc);
     } else {
+        // protein has no reverse strand: rc stays empty and is still "extended"
+        // (executor.rs:633-637, 693-697)
         fok = extend_chains(tg, cfg, read, len, fchains, &fsc);
-        rok = extend_chains(tg, cfg, rc.data(), len, rchains, &rsc);
+        rok = extend_chains(tg, cfg, rc.data(), rc.size(), rchains, &rsc);
     }
     if (fok && rok && rsc.primary.ed < fsc.primary.ed) {
         out->scored = std::move(rsc);

@@ -196,3 +196,150 @@ def myers_edit_distance(query, target):
     """myers_edit_distance (lib.rs:94-96) -> (edit_distance, cigar)."""
     r = default_engine().extend(A.ENGINE_MYERS_GLOBAL, [(bytes(query), bytes(target))])[0]
     return r[2], r[1]
+
+
+# ---------------------------------------------------------------------------
+# Target index, sketching, seeding/chaining and align_read
+# ---------------------------------------------------------------------------
+class Index:
+    """TargetContext on the device (phr_index): target bytes, minimizer index, cap."""
+
+    def __init__(self, engine, target, alphabet=A.ALPHABET_DNA, sketch=None):
+        self._eng = engine
+        self._lib = engine._lib
+        target = bytes(target)
+        h = C.c_void_p()
+        sk = None
+        if sketch is not None:
+            vals = np.ascontiguousarray(sketch[0], dtype=np.uint64)
+            pos = np.ascontiguousarray(sketch[1], dtype=np.uint32)
+            self._keep = (vals, pos)
+            sk = A.Sketch(vals.ctypes.data, pos.ctypes.data, len(vals), 0, 0)
+        engine.check(self._lib.phr_index_create(engine.handle, target, len(target),
+                                                C.byref(sk) if sk is not None else None, alphabet, C.byref(h)))
+        self._h = h
+        self.alphabet = alphabet
+        self.target = target
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        inf = A.IndexInfo()
+        self._eng.check(self._lib.phr_index_get_info(self._h, C.byref(inf)))
+        return {"n_minimizers": inf.n_minimizers, "n_distinct": inf.n_distinct,
+                "occurrence_cap": inf.occurrence_cap, "target_len": inf.target_len,
+                "device_bytes": inf.device_bytes}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.phr_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _sketch(engine, seqs, k, w, alphabet):
+    from .batch import PackedReads
+    packed = PackedReads(seqs)
+    caps = np.maximum(packed.len.astype(np.int64) - k + 1, 0).astype(np.uint64)
+    out_off = np.zeros(packed.n, dtype=np.uint64)
+    if packed.n > 1:
+        np.cumsum(caps[:-1], out=out_off[1:])
+    tot = int(caps.sum()) + 1
+    vals = np.zeros(tot, dtype=np.uint64)
+    pos = np.zeros(tot, dtype=np.uint32)
+    cnt = np.zeros(max(packed.n, 1), dtype=np.uint32)
+    sb = A.SeqBatch(packed.n, packed.seq.ctypes.data, packed.seq.nbytes, packed.off.ctypes.data,
+                    packed.len.ctypes.data)
+    engine.check(engine._lib.phr_sketch_batch(engine.handle, C.byref(sb), k, w, alphabet, out_off.ctypes.data,
+                                              vals.ctypes.data, pos.ctypes.data, cnt.ctypes.data))
+    return [(vals[o:o + c].copy(), pos[o:o + c].copy()) for o, c in zip(out_off.tolist(), cnt.tolist())]
+
+
+def _seed_chain(engine, index, sketches):
+    n = len(sketches)
+    keep = []
+    sk = (A.Sketch * max(n, 1))()
+    total = 0
+    for i, (v, p) in enumerate(sketches):
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        p = np.ascontiguousarray(p, dtype=np.uint32)
+        keep.append((v, p))
+        sk[i] = A.Sketch(v.ctypes.data if len(v) else None, p.ctypes.data if len(p) else None, len(v), 0, 0)
+        total += len(v)
+    cap = total * int(index.info()["occurrence_cap"]) + 16
+    cap = min(cap, 1 << 26)
+    nsf = np.zeros(max(n, 1), np.uint32)
+    nch = np.zeros(max(n, 1), np.uint32)
+    coff = np.zeros(max(n, 1), np.uint64)
+    chains = np.zeros(cap, dtype=np.dtype([("score", "<i8"), ("seed_off", "<u4"), ("n_seeds", "<u4"),
+                                           ("target_start", "<u4"), ("_pad", "<u4")]))
+    seeds = np.zeros(cap, dtype=np.dtype([("query_pos", "<u4"), ("target_pos", "<u4"), ("minimizer", "<u8")]))
+    arena = A.ChainArena(nsf.ctypes.data, nch.ctypes.data, coff.ctypes.data, chains.ctypes.data, cap,
+                         seeds.ctypes.data, cap)
+    engine.check(engine._lib.phr_seed_chain_batch(engine.handle, index.handle, sk, n, C.byref(arena)))
+    out = []
+    for u in range(n):
+        cl = []
+        for c in chains[int(coff[u]):int(coff[u]) + int(nch[u])]:
+            ss = [(int(s["query_pos"]), int(s["target_pos"]), int(s["minimizer"]))
+                  for s in seeds[c["seed_off"]:c["seed_off"] + c["n_seeds"]]]
+            cl.append((int(c["score"]), int(c["target_start"]), ss))
+        out.append((int(nsf[u]), cl))
+    return out
+
+
+def _align_packed(engine, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE):
+    n = packed.n
+    rr = np.zeros(max(n, 1), dtype=READ_RESULT_DTYPE)
+    K = 1 if strategy == A.FAST else 2 if strategy == A.BALANCED else 50
+    acap = 2 * K * n + 16
+    aln = np.zeros(acap, dtype=ALN_DTYPE)
+    maxlen = int(packed.len.max()) if n else 1
+    ccap = int(acap) * (6 * maxlen + 16)
+    ccap = min(ccap, 1 << 31)
+    cig = np.zeros(ccap, dtype=np.uint8)
+    arena = A.ReadResultArena(rr.ctypes.data, aln.ctypes.data, acap, 0, cig.ctypes.data, ccap, 0)
+    stats = A.AlignStats()
+    cfg = A.AlignConfig(strategy, gap_model)
+    b = packed.batch()
+    engine.check(engine._lib.phr_align_reads(engine.handle, index.handle, C.byref(b), C.byref(cfg), C.byref(arena),
+                                             C.byref(stats)))
+    st = (stats.placed, stats.no_seed, stats.below_threshold, stats.fast_cutoff, stats.no_alignment)
+    return rr[:n], aln[:arena.aln_used], cig[:arena.cigar_used], st
+
+
+def unpack_reads(rr, aln, cig):
+    """-> [(outcome, has_result, reverse, [(cigar, ed, qs, qe, ts, te), ...])]"""
+    out = []
+    cb = bytes(cig)
+    for r in rr:
+        alns = []
+        for j in range(int(r["aln_off"]), int(r["aln_off"]) + int(r["n_aln"])):
+            a = aln[j]
+            s = cb[a["cigar_off"]:a["cigar_off"] + a["cigar_len"]].decode()
+            alns.append((s, int(a["edit_distance"]), int(a["query_start"]), int(a["query_end"]),
+                         int(a["target_start"]), int(a["target_end"])))
+        out.append((int(r["outcome"]), int(r["has_result"]), int(r["reverse"]), alns))
+    return out
+
+
+def _engine_index(self, target, alphabet=A.ALPHABET_DNA, sketch=None):
+    return Index(self, target, alphabet, sketch)
+
+
+def _engine_align_reads(self, index, reads, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, stored=None):
+    packed = reads if isinstance(reads, PackedReads) else PackedReads(reads, stored)
+    rr, aln, cig, st = _align_packed(self, index, packed, strategy, gap_model)
+    return unpack_reads(rr, aln, cig), st
+
+
+Engine.index = _engine_index
+Engine.align_reads = _engine_align_reads
+Engine.align_packed = lambda self, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE: _align_packed(
+    self, index, packed, strategy, gap_model)
+Engine.sketch = lambda self, seqs, k=21, w=11, alphabet=A.ALPHABET_DNA: _sketch(self, seqs, k, w, alphabet)
+Engine.seed_chain = lambda self, index, sketches: _seed_chain(self, index, sketches)

@@ -8,10 +8,6 @@
 
 using phr::Ctx;
 
-struct phr_ctx {
-    Ctx impl;
-};
-
 namespace {
 
 phr_status check_ctx(phr_ctx* c) { return c ? PHR_OK : PHR_ERR_ARG; }

@@ -235,7 +235,7 @@ __global__ void pack_kernel(PackParams P) {
         return;
     }
     const uint8_t* qsrc = P.in.seq + P.in.q_off[i] + d.qs;
-    const uint8_t* tsrc = P.in.seq + P.in.t_off[i] + d.ts;
+    const uint8_t* tsrc = (P.in.t_seq ? P.in.t_seq : P.in.seq) + P.in.t_off[i] + d.ts;
     const uint64_t w2 = P.w2_off[i];
     const uint64_t q2w = (d.qn + 15) / 16 + 4;
     bool pure = true;

@@ -41,6 +41,8 @@ struct Ctx {
     DeviceArena arena;       // per-call temporaries
     DeviceArena scratch;     // per-warp slots of the persistent kernels
     DeviceArena io;          // device copies of host inputs / outputs
+    DeviceArena pipe;        // align_read pipeline state (kept across its extension calls)
+    DeviceArena seeds;       // per-seed arrays of seeding/chaining, sized from the exact seed count
     size_t scratch_budget = 8ull << 30;
     std::string last_error;
     std::atomic<uint64_t> launches{0};
@@ -89,6 +91,7 @@ struct DevPairs {
     const uint32_t* t_len = nullptr;
     const uint32_t* q_seed = nullptr;
     const uint32_t* t_seed = nullptr;
+    const uint8_t* t_seq = nullptr;   // when set, targets are read from this arena instead of seq
 };
 
 // Device-resident output of a pair batch.
@@ -122,3 +125,8 @@ void launch_wfa_linear_bytes(const ExtendParams& p, int grid, int block, cudaStr
 void launch_wfa_affine_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st);
 
 }  // namespace phr
+
+// The opaque context handle of the C ABI.
+struct phr_ctx {
+    phr::Ctx impl;
+};

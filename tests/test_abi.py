@@ -1,0 +1,52 @@
+"""CPU checks of the C ABI: the library loads and exports every declared entry point,
+and the ctypes mirror matches the header's struct layouts."""
+import ctypes as C
+import os
+import re
+
+from phraya_b200 import _abi as A
+from phraya_b200 import api as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    hdr = open(os.path.join(ROOT, "include", "phraya_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(phr_[a-z_]+)\s*\(", hdr)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = P.lib()
+    names = declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(names) == set(A.PROTOTYPES), set(names) ^ set(A.PROTOTYPES)
+    assert L.phr_abi_version() == 1
+
+
+def test_struct_sizes_match_header_layout():
+    assert C.sizeof(A.Alignment) == 40
+    assert C.sizeof(A.PairBatch) == 72
+    assert C.sizeof(A.ReadResult) == 24
+    assert C.sizeof(A.Chain) == 24
+    assert C.sizeof(A.Seed) == 16
+    assert C.sizeof(A.KernelTiming) == 48
+
+
+def test_no_device_means_engine_unavailable():
+    # on a machine without a GPU the context refuses to open (there is no CPU path)
+    import torch
+    if torch.cuda.is_available():
+        return
+    try:
+        P.Engine(0)
+    except P.EngineUnavailable:
+        return
+    raise AssertionError("Engine opened without a CUDA device")
+
+
+def test_status_strings():
+    L = P.lib()
+    for s in range(9):
+        assert L.phr_status_string(s)
