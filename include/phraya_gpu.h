@@ -312,7 +312,8 @@ typedef enum {
 /*
  * Per read: the winning orientation's ScoredAlignments (primary first, then the
  * alternatives with score ratio >= 0.95, lib.rs:170-199) as alignments
- * aln[aln_off .. aln_off + n_aln); `reverse` = 1 when the reverse complement won.
+ * aln[aln_off .. aln_off + n_aln); `reverse` = 1 when the reverse complement won
+ * (0 whenever has_result = 0).
  * has_result = 0 when align_read would return None (NoAlignment, FastCutoff, stored
  * empty sketch); `outcome` is always set. query_positions of the reference
  * (executor.rs:777-781) are (aln.target_start, 1 - aln.edit_distance / max(|q|,1)).

@@ -1200,6 +1200,7 @@ void align_read(const Target& tg, const uint8_t* read, size_t len, const phr_ali
         if (div > 0.20) {
             out->outcome = PHR_OUT_FAST_CUTOFF;
             out->has_result = false;
+            out->reverse = false;  // no result: orientation is not reported
             return;
         }
     }

@@ -498,6 +498,8 @@ struct GateArgs {
     int8_t* ou_engine;             // -1: not extended
     uint32_t* ou_count;
     int32_t* read_early;           // -1 none, else outcome (NoSeed for stored-empty)
+    uint8_t* had_seeds;            // per read: a seed in either searched orientation
+    uint8_t* rev_searched;         // per read: reverse orientation seeded and chained
     uint32_t* eng_count;           // [slot * (n_reads + 1) + read] pair counts, for the scans
 };
 
@@ -515,8 +517,13 @@ __global__ void gate_kernel(GateArgs G) {
     const bool dna = G.alphabet == PHR_ALPHABET_DNA;
     const uint64_t uf = r, ur = G.n_reads + r;
     const uint32_t fs = G.nseeds[uf];
-    const uint32_t rs = dna ? G.nseeds[ur] : 0;
+    // executor.rs:641-643: an empty forward sketch that found no seeds skips the
+    // reverse orientation entirely (no reverse seeds, no reverse chains)
+    const bool rev_searched = dna && !(fs == 0 && G.sk_n[uf] == 0);
+    const uint32_t rs = rev_searched ? G.nseeds[ur] : 0;
     const bool had_seeds = fs > 0 || rs > 0;
+    G.had_seeds[r] = had_seeds ? 1 : 0;
+    G.rev_searched[r] = rev_searched ? 1 : 0;
     const bool stored = G.has_stored && G.has_stored[r];
     const uint64_t stride = G.n_reads + 1;
     G.eng_count[r] = G.eng_count[stride + r] = G.eng_count[2 * stride + r] = 0;
@@ -528,7 +535,7 @@ __global__ void gate_kernel(GateArgs G) {
         return;
     }
     const uint32_t fc = G.nchains[uf];
-    const uint32_t rc = dna ? G.nchains[ur] : 0;
+    const uint32_t rc = rev_searched ? G.nchains[ur] : 0;
     const bool ext_f = !(fc == 0 && rc > 0);
     const bool ext_r = !(fc > 0 && rc == 0);
     const uint32_t len_o[2] = {G.len[r], dna ? G.len[r] : 0u};
@@ -555,6 +562,7 @@ struct PairBuildArgs {
     const uint64_t* read_off;      // fwd reads in the query arena
     const uint64_t* rc_off;        // rc reads in the query arena
     const uint32_t* len;
+    const uint8_t* rev_searched;   // per read
     int alphabet;
     uint64_t target_len;
     // per engine slot pair arrays
@@ -577,7 +585,7 @@ __global__ void pair_build_kernel(PairBuildArgs B) {
         if (e < 0) continue;
         const int es = eng_slot(e);
         const uint64_t u = o == 0 ? r : B.n_reads + r;
-        const uint32_t nc = (o == 1 && !dna) ? 0u : B.nchains[u];
+        const uint32_t nc = (o == 1 && !B.rev_searched[r]) ? 0u : B.nchains[u];
         const uint32_t cnt = B.ou_count[2 * r + o];
         const uint32_t qlen = (o == 1 && !dna) ? 0u : B.len[r];
         const uint64_t qo = o == 0 ? B.read_off[r] : B.rc_off[r];
@@ -602,7 +610,7 @@ struct SelectArgs {
     uint64_t n_reads;
     int alphabet, strategy;
     const uint32_t* len;
-    const uint32_t* nseeds;
+    const uint8_t* had_seeds;
     const int32_t* read_early;
     const int8_t* ou_engine;
     const uint32_t* ou_count;
@@ -630,7 +638,7 @@ __global__ void select_kernel(SelectArgs S) {
     phr_read_result out;
     memset(&out, 0, sizeof(out));
     const bool dna = S.alphabet == PHR_ALPHABET_DNA;
-    const bool had_seeds = S.nseeds[r] > 0 || (dna && S.nseeds[S.n_reads + r] > 0);
+    const bool had_seeds = S.had_seeds[r] != 0;
     uint64_t* list = S.sel_pair + r * S.sel_cap;
     if (S.read_early[r] >= 0) {
         out.outcome = S.read_early[r];
@@ -1247,6 +1255,8 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
     G.ou_engine = static_cast<int8_t*>(A.take(2 * n + 8));
     G.ou_count = static_cast<uint32_t*>(A.take(2 * n * 4 + 8));
     G.read_early = static_cast<int32_t*>(A.take(n * 4 + 8));
+    G.had_seeds = static_cast<uint8_t*>(A.take(n + 8));
+    G.rev_searched = static_cast<uint8_t*>(A.take(n + 8));
     G.eng_count = static_cast<uint32_t*>(A.take(3 * stride * 4 + 16));
     uint64_t* cnt64 = static_cast<uint64_t*>(A.take(3 * stride * 8 + 16));
     uint64_t* eng_first = static_cast<uint64_t*>(A.take(3 * stride * 8 + 16));
@@ -1286,6 +1296,7 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
     PB.read_off = rd_off;
     PB.rc_off = rc_off;
     PB.len = d_len;
+    PB.rev_searched = G.rev_searched;
     PB.alphabet = idx->alphabet;
     PB.target_len = idx->target_len;
     PB.ou_first = ou_first;
@@ -1354,7 +1365,7 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
     SA.alphabet = idx->alphabet;
     SA.strategy = cfg.strategy;
     SA.len = d_len;
-    SA.nseeds = C.nseeds;
+    SA.had_seeds = G.had_seeds;
     SA.read_early = G.read_early;
     SA.ou_engine = G.ou_engine;
     SA.ou_count = G.ou_count;
