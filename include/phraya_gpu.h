@@ -173,6 +173,41 @@ phr_status phr_extend_batch_device(phr_ctx* ctx, phr_engine engine, const phr_pa
 phr_status phr_extend_percall(phr_ctx* ctx, phr_engine engine, const phr_pair_batch* batch,
                               phr_affine_costs costs, phr_result_arena* out);
 
+/*
+ * Allocation-free Myers fitting extension. No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory: code running next to a caching
+ * allocator that already holds the device's memory (where a cudaMalloc of its own can
+ * fail or fragment that pool), and latency-critical loops that cannot afford the
+ * implicit device-wide synchronisation cudaMalloc/cudaFree may bring. It computes
+ * exactly what phr_extend_batch(PHR_ENGINE_MYERS_FIT) computes (myers_extend with the
+ * anchor at (0, 0), phraya-align/src/lib.rs:106-127), but every byte of scratch it
+ * needs lives in one fixed array inside the library (PHR_NOALLOC_SCRATCH_BYTES of
+ * device memory, held by each GPU that loads the library until the process exits).
+ *
+ * All pointers are DEVICE memory owned by the caller: pair i aligns
+ * seq[q_off[i] .. +q_len[i]) against seq[t_off[i] .. +t_len[i]); results go to
+ * status[i], edit_distance[i], target_consumed[i], cigar_len[i] and the CIGAR text at
+ * cigar + i * cigar_stride. `stream` is a cudaStream_t (NULL = default stream); the call
+ * returns after the work on it has finished.
+ * Limits: |q| <= PHR_NOALLOC_MAX_QUERY, |t| <= PHR_NOALLOC_MAX_TARGET (the reference's
+ * Myers regime: queries of at most 500 bases against windows of twice that); longer
+ * pairs get status PHR_ERR_ARG and the call returns PHR_ERR_ARG. cigar_stride must be at
+ * least PHR_NOALLOC_CIGAR_STRIDE.
+ * The first call on a device looks up the scratch array's device address (once per
+ * device, with that device current); make that first call before any stream capture.
+ * Every call shares the one scratch array, so calls that overlap on the GPU (other
+ * streams, other host threads) race: serialise them.
+ */
+#define PHR_NOALLOC_MAX_QUERY 512u
+#define PHR_NOALLOC_MAX_TARGET 1024u
+#define PHR_NOALLOC_CIGAR_STRIDE 3072u
+#define PHR_NOALLOC_SCRATCH_BYTES (64ull << 20)
+phr_status phr_myers_extend_noalloc(const uint8_t* seq, const uint64_t* q_off, const uint32_t* q_len,
+                                    const uint64_t* t_off, const uint32_t* t_len, uint64_t n_pairs,
+                                    int32_t* status, uint32_t* edit_distance, uint32_t* target_consumed,
+                                    char* cigar, uint32_t cigar_stride, uint32_t* cigar_len, void* stream);
+
 /* ------------------------------------------------------------------------- */
 /* Sketches, target index, seeding and chaining                               */
 /* ------------------------------------------------------------------------- */

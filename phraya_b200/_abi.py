@@ -260,6 +260,9 @@ PROTOTYPES = {
     "phr_server_poll": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
     "phr_server_destroy": (C.c_int32, [C.c_void_p]),
+    "phr_myers_extend_noalloc": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                             C.c_void_p, C.c_void_p]),
 }
 
 

@@ -22,6 +22,8 @@
 // a band |i - j| <= E + 2 are stored: every cell of an alignment of cost ed satisfies
 // |i - j| <= ed, so the walk stays in the band whenever ed <= E; pairs with ed > E are
 // redone with every block stored (full_band).
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace phr {
@@ -454,3 +456,212 @@ void launch_myers_bytes(const ExtendParams& p, int grid, int block, cudaStream_t
 }
 
 }  // namespace phr
+
+// ===========================================================================
+// Allocation-free Myers fitting extension (phr_myers_extend_noalloc).
+//
+// Its scratch is the file-scope array below: 256 bytes of control words (pair counter,
+// error flags) followed by one fixed slice per worker warp. A slice holds the pair's
+// bookkeeping header, both sequences copied into word-aligned staging, and the
+// full-band records + runs myers_group needs; the length limits make every pair fit
+// its slice, so no redo pass (and no allocation) is ever needed.
+// ===========================================================================
+namespace phr {
+namespace {
+
+constexpr int kNoAllocWarps = 128;
+constexpr uint64_t kNoAllocCtl = 256;
+constexpr uint64_t kNoAllocSlice = (PHR_NOALLOC_SCRATCH_BYTES - kNoAllocCtl) / kNoAllocWarps / 256 * 256;
+constexpr uint64_t kNoAllocHeader = 256;
+constexpr uint64_t kNoAllocStageQ = (PHR_NOALLOC_MAX_QUERY / 4 + 8) * 4;
+constexpr uint64_t kNoAllocStageT = (PHR_NOALLOC_MAX_TARGET / 4 + 8) * 4;
+constexpr uint64_t kNoAllocWork = kNoAllocHeader + kNoAllocStageQ + kNoAllocStageT;
+// worst pair: full band of ceil(512/64) = 8 blocks x 1024 columns x 32 B + runs
+static_assert(kNoAllocWork + 1024ull * 8 * 32 + (1024 + 512 + 2) * 4 + 64 <= kNoAllocSlice,
+              "no-alloc slice too small for the stated limits");
+
+struct NoAllocArgs {
+    const uint8_t* seq;
+    const uint64_t* q_off;
+    const uint32_t* q_len;
+    const uint64_t* t_off;
+    const uint32_t* t_len;
+    uint64_t n;
+    int32_t* status;
+    uint32_t* ed;
+    uint32_t* consumed;
+    char* cigar;
+    uint32_t stride;
+    uint32_t* cigar_len;
+    uint8_t* scratch;    // device address of g_noalloc_scratch
+};
+
+__device__ uint32_t noalloc_write_count_op(char* p, uint32_t n, char op) {
+    const uint32_t nd = ndigits(n);
+    for (int d = static_cast<int>(nd) - 1; d >= 0; --d) {
+        p[d] = static_cast<char>('0' + n % 10);
+        n /= 10;
+    }
+    p[nd] = op;
+    return nd + 1;
+}
+
+__global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
+    const int lane = lane_id();
+    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    uint32_t* ctl = reinterpret_cast<uint32_t*>(A.scratch);  // [0] next pair, [1] error flags
+    uint8_t* slice = A.scratch + kNoAllocCtl + w * kNoAllocSlice;
+    PairOut* pout = reinterpret_cast<PairOut*>(slice);
+    uint64_t* toff = reinterpret_cast<uint64_t*>(slice + 64);
+    uint32_t* err = reinterpret_cast<uint32_t*>(slice + 72);
+    uint32_t* rcount = reinterpret_cast<uint32_t*>(slice + 76);
+    unsigned long long* rneed = reinterpret_cast<unsigned long long*>(slice + 80);
+    uint32_t* rlist = reinterpret_cast<uint32_t*>(slice + 88);
+    uint32_t* stage = reinterpret_cast<uint32_t*>(slice + kNoAllocHeader);
+    uint8_t* work = slice + kNoAllocWork;
+    for (;;) {
+        uint64_t i = 0;
+        if (lane == 0) i = atomicAdd(reinterpret_cast<unsigned long long*>(ctl + 2), 1ull);
+        i = __shfl_sync(PHR_FULL_MASK, i, 0);
+        if (i >= A.n) break;
+        const uint32_t ql = A.q_len[i], tl = A.t_len[i];
+        char* text = A.cigar + i * A.stride;
+        if (ql > PHR_NOALLOC_MAX_QUERY || tl > PHR_NOALLOC_MAX_TARGET) {
+            if (lane == 0) {
+                A.status[i] = PHR_ERR_ARG;
+                A.ed[i] = 0;
+                A.consumed[i] = 0;
+                A.cigar_len[i] = 0;
+                atomicOr(ctl + 1, 1u);
+            }
+            continue;
+        }
+        if (ql == 0 || tl == 0) {  // wfa_simd.rs:3793-3798
+            if (lane == 0) {
+                A.status[i] = PHR_OK;
+                A.ed[i] = ql;
+                A.consumed[i] = 0;
+                A.cigar_len[i] = ql ? noalloc_write_count_op(text, ql, 'D') : 0;
+            }
+            continue;
+        }
+        // word-aligned staging of both sequences (byte mode: 4 symbols per word)
+        const uint32_t qw = (ql + 3) / 4 + 4;
+        const uint8_t* qs = A.seq + A.q_off[i];
+        const uint8_t* ts = A.seq + A.t_off[i];
+        for (uint32_t k = lane; k < qw; k += 32) {
+            uint32_t word = 0;
+            for (uint32_t b = 0; b < 4; ++b) {
+                const uint32_t p = 4 * k + b;
+                if (p < ql) word |= static_cast<uint32_t>(qs[p]) << (8 * b);
+            }
+            stage[k] = word;
+        }
+        const uint32_t tw = (tl + 3) / 4 + 4;
+        for (uint32_t k = lane; k < tw; k += 32) {
+            uint32_t word = 0;
+            for (uint32_t b = 0; b < 4; ++b) {
+                const uint32_t p = 4 * k + b;
+                if (p < tl) word |= static_cast<uint32_t>(ts[p]) << (8 * b);
+            }
+            stage[qw + k] = word;
+        }
+        if (lane == 0) {
+            *toff = i * A.stride;
+            *err = 0;
+            *rcount = 0;
+            *rneed = 0;
+            PairOut o = {};
+            o.status = -1;
+            *pout = o;
+        }
+        __syncwarp();
+        ExtendParams P{};
+        P.out = pout;
+        P.bytes = stage;
+        P.packed2 = stage;
+        P.text = A.cigar;
+        P.text_off = toff;
+        P.redo_list = rlist;
+        P.redo_count = rcount;
+        P.redo_need_max = rneed;
+        P.engine = PHR_ENGINE_MYERS_FIT;
+        P.full_band = 1;
+        P.band_base = 0;
+        P.error_flag = err;
+        PairDesc d = {};
+        d.q_word = 0;
+        d.t_word = qw;
+        d.qn = static_cast<int32_t>(ql);
+        d.tn = static_cast<int32_t>(tl);
+        d.mode = 1;
+        int G = 1;
+        const int nb = static_cast<int>((ql + 63) / 64);
+        while (G < nb) G <<= 1;
+        myers_group<SeqB>(P, d, 0, lane < G, G, work, 0, true);
+        __syncwarp();
+        if (lane == 0) {
+            const PairOut o = *pout;
+            const bool ok = o.status == PHR_OK && *err == 0 && *rcount == 0;
+            A.status[i] = ok ? PHR_OK : PHR_ERR_CUDA;
+            A.ed[i] = ok ? static_cast<uint32_t>(o.ed) : 0;
+            A.consumed[i] = ok ? static_cast<uint32_t>(o.t_consumed) : 0;
+            A.cigar_len[i] = ok ? o.text_len : 0;
+            if (!ok) atomicOr(ctl + 1, 2u);
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+// One fixed scratch array per GPU that loads the library.
+static __device__ __align__(256) uint8_t g_noalloc_scratch[PHR_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch for the current device, looked up once per device.
+static cudaError_t noalloc_scratch_address(uint8_t** out) {
+    static std::mutex mu;
+    static uint8_t* addr[256] = {nullptr};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = static_cast<uint8_t*>(p);
+    }
+    *out = addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace phr
+
+extern "C" phr_status phr_myers_extend_noalloc(const uint8_t* seq, const uint64_t* q_off, const uint32_t* q_len,
+                                               const uint64_t* t_off, const uint32_t* t_len, uint64_t n_pairs,
+                                               int32_t* status, uint32_t* edit_distance, uint32_t* target_consumed,
+                                               char* cigar, uint32_t cigar_stride, uint32_t* cigar_len,
+                                               void* stream) {
+    if (n_pairs == 0) return PHR_OK;
+    if (!seq || !q_off || !q_len || !t_off || !t_len || !status || !edit_distance || !target_consumed || !cigar ||
+        !cigar_len)
+        return PHR_ERR_ARG;
+    if (cigar_stride < PHR_NOALLOC_CIGAR_STRIDE) return PHR_ERR_ARG;
+    uint8_t* scratch = nullptr;
+    if (phr::noalloc_scratch_address(&scratch) != cudaSuccess) return PHR_ERR_CUDA;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the control words (pair counter, error flags) must start at zero on every call
+    if (cudaMemsetAsync(scratch, 0, phr::kNoAllocCtl, st) != cudaSuccess) return PHR_ERR_CUDA;
+    phr::NoAllocArgs A{seq, q_off, q_len, t_off, t_len, n_pairs, status, edit_distance, target_consumed,
+                       cigar, cigar_stride, cigar_len, scratch};
+    phr::myers_noalloc_kernel<<<phr::kNoAllocWarps * 32 / 256, 256, 0, st>>>(A);
+    if (cudaGetLastError() != cudaSuccess) return PHR_ERR_CUDA;
+    uint32_t flags = 0;
+    if (cudaMemcpyAsync(&flags, scratch + 4, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PHR_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PHR_ERR_CUDA;
+    if (flags & 2u) return PHR_ERR_CUDA;
+    if (flags & 1u) return PHR_ERR_ARG;
+    return PHR_OK;
+}
