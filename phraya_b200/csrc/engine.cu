@@ -333,9 +333,9 @@ __global__ void task_flag_kernel(TaskBuild T) {
 
 __device__ __forceinline__ uint64_t myers_need_est(int m, int n, int G, int band_base) {
     const int nb = (m + 63) >> 6;
-    int E = min(band_base + abs(m - n) + (m >> 3), max(m, n));
+    int E = min(band_base + abs(m - n) + (m >> 4), max(m, n));
     int W = min((2 * (E + 2) + 1 + 63) / 64 + 1, nb);
-    uint64_t need = ((static_cast<uint64_t>(n) * W * 32) + 15) & ~15ull;
+    uint64_t need = ((static_cast<uint64_t>(n) * W * 16) + 15) & ~15ull;  // 16-byte VP/HP records
     if (nb > G) need += (static_cast<uint64_t>(n) + 15) & ~15ull;
     need += (static_cast<uint64_t>(m + n + 2) * 4 + 15) & ~15ull;
     return need;

@@ -16,9 +16,9 @@
 // The reference reconstructs whole DP columns from VP/VN during traceback. Its
 // decisions only need two delta bits per cell: `cur == above + 1` is VP(i-1) of
 // column j and `cur == left + 1` is HP(i-1) (the horizontal delta the forward pass
-// already computes); a diagonal move is a match iff -VN(i-1) + dh(i-1, j) == 0, with
-// dh(0, j) = 1 (top row D[0][j] = j). So the forward pass stores {VP, VN, HP, HN} per
-// (column, block) and the traceback walks bits, never values. Only the blocks within
+// already computes); a diagonal move is M or X by comparing the two bytes, exactly as
+// the reference does. So the forward pass stores {VP, HP} per (column, block) and the
+// traceback walks bits, never values. Only the blocks within
 // a band |i - j| <= E + 2 are stored: every cell of an alignment of cost ed satisfies
 // |i - j| <= ed, so the walk stays in the band whenever ed <= E; pairs with ed > E are
 // redone with every block stored (full_band).
@@ -29,7 +29,7 @@
 namespace phr {
 namespace {
 
-constexpr int kRecBytes = 32;  // VP, VN, HP, HN of one 64-bit block of one column
+constexpr int kRecBytes = 16;  // VP and HP of one 64-bit block of one column
 
 __device__ __forceinline__ uint32_t compress_even(uint32_t x) {
     x &= 0x55555555u;
@@ -60,7 +60,7 @@ __device__ __forceinline__ Band make_band(int m, int n, int nb, int full, int ba
         b.E = max(m, n);
         b.W = nb;
     } else {
-        int E = base + abs(m - n) + (m >> 3);
+        int E = base + abs(m - n) + (m >> 4);
         E = min(E, max(m, n));
         b.E = E;
         int W = (2 * (E + 2) + 1 + 63) / 64 + 1;
@@ -135,6 +135,30 @@ __device__ __forceinline__ const uint32_t* seq_base(const ExtendParams& P, uint6
     return (S::kBits == 2 ? P.packed2 : P.bytes) + word;
 }
 
+// 64-bit a + b + carry_in with carry out (one add chain).
+__device__ __forceinline__ uint64_t add_carry64(uint64_t a, uint64_t b, uint32_t cin, uint32_t* cout) {
+    uint32_t lo, hi, c;
+    const uint32_t alo = static_cast<uint32_t>(a), ahi = static_cast<uint32_t>(a >> 32);
+    const uint32_t blo = static_cast<uint32_t>(b), bhi = static_cast<uint32_t>(b >> 32);
+    asm("{\n\t"
+        ".reg .u32 t;\n\t"
+        "add.cc.u32 t, %5, 0xFFFFFFFF;\n\t"  // carry flag := (cin != 0)
+        "addc.cc.u32 %0, %3, %4;\n\t"
+        "addc.cc.u32 %1, %6, %7;\n\t"
+        "addc.u32 %2, 0, 0;\n\t"
+        "}"
+        : "=r"(lo), "=r"(hi), "=r"(c)
+        : "r"(alo), "r"(blo), "r"(cin), "r"(ahi), "r"(bhi));
+    *cout = c;
+    return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+// Bit r (window row offset 0..127) of the 128-bit word hi:lo.
+__device__ __forceinline__ uint32_t bit128(uint64_t lo, uint64_t hi, int r) {
+    const uint64_t w = r >= 64 ? hi : lo;
+    return static_cast<uint32_t>((w >> (r & 63)) & 1ull);
+}
+
 // Runs one Myers alignment per active group of the warp. All 32 lanes call this with
 // warp-uniform control flow; `act` marks lanes whose group holds a pair.
 template <class S>
@@ -149,7 +173,6 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
     const Band band = make_band(m, n, nb, P.full_band, P.band_base);
     const uint32_t* qb = seq_base<S>(P, d.q_word);
     const uint32_t* tb = seq_base<S>(P, d.t_word);
-    const int qsh = 0, tsh = 0;
 
     uint8_t* recs = slot + slot_off;
     uint64_t off = align16(static_cast<uint64_t>(n) * band.W * kRecBytes);
@@ -161,105 +184,101 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
     const int R = go ? (nb + G - 1) / G : 0;
     const int Rmax = __reduce_max_sync(PHR_FULL_MASK, static_cast<unsigned>(R));
     const int last_lane = (nb - 1) % G;
-    const uint64_t last_mask = (m & 63) ? ((1ull << (m & 63)) - 1) : ~0ull;
     const int score_bit = (m - 1) & 63;
     const int margin = m / 10 + 1;
+    const bool any_fit = __any_sync(PHR_FULL_MASK, fitting);
 
-    int score = m, best = m, best_col = 0, ncols = n;
+    int score = m, best = m, best_col = 0;
     bool stopped = false;
+    int colsum = 0;  // global mode: sum of VP - VN bits of the final column (rows < m)
 
+    // ---- forward pass: anti-diagonal lane pipeline -------------------------------
+    // Bits at or above m in the last block are never masked: carries and shifts only move
+    // upward, so they cannot reach a bit below m, and nothing above m is ever read.
     for (int r = 0; r < Rmax; ++r) {
         const int blk = r * G + gl;
         const bool blk_act = go && r < R && blk < nb;
-        const bool is_last = blk_act && blk == nb - 1;
-        const uint64_t bmask = (blk == nb - 1) ? last_mask : ~0ull;
+        const uint64_t smask = (blk_act && blk == nb - 1) ? (1ull << score_bit) : 0ull;
         QueryBlock<S> qbk;
-        if (blk_act) qbk.load(qb, qsh, blk, bmask);
-        uint64_t vp = bmask, vn = 0;
+        if (blk_act) qbk.load(qb, 0, blk, ~0ull);
+        uint64_t vp = ~0ull, vn = 0;
         const int steps = (go && r < R) ? n + G - 1 : 0;
         const int smax = __reduce_max_sync(PHR_FULL_MASK, static_cast<unsigned>(steps));
         uint32_t payload = 0;
+        uint32_t tword = 0;
         bool stop_r = false;
+        // first stored block of column J = j0 + 1, tracked incrementally (Band::blo)
+        int blo_cur = band.blo(1 - gl > 1 ? 1 - gl : 1);
         for (int s = 0; s < smax; ++s) {
-            const uint32_t in = __shfl_up_sync(PHR_FULL_MASK, payload, 1, G);
+            uint32_t in = __shfl_up_sync(PHR_FULL_MASK, payload, 1, G);
             const int j0 = s - gl;
             const bool live = blk_act && j0 >= 0 && j0 < n && !stop_r;
+            // every lane keeps the group's current target word; only lane 0 reads it
+            if ((s % S::kPerWord) == 0 && s < n && go) tword = __ldg(tb + s / S::kPerWord);
             if (live) {
-                uint32_t c, addc, hpc, hnc;
                 if (gl == 0) {
-                    c = sym_at<S>(tb, j0 + tsh);
-                    if (r == 0) {
-                        addc = 0;
-                        hpc = 1;
-                        hnc = 0;
-                    } else {
-                        const uint32_t cb = stripe_buf[j0];
-                        addc = cb & 1;
-                        hpc = (cb >> 1) & 1;
-                        hnc = (cb >> 2) & 1;
-                    }
-                } else {
-                    c = in & 0xffu;
-                    addc = (in >> 8) & 1;
-                    hpc = (in >> 9) & 1;
-                    hnc = (in >> 10) & 1;
+                    // lane 0: target symbol j0 and the carries entering block 0 of the stripe
+                    const uint32_t c0 = (tword >> ((s % S::kPerWord) * S::kBits)) & ((1u << S::kBits) - 1);
+                    const uint32_t cb = r == 0 ? 2u : static_cast<uint32_t>(stripe_buf[j0]);
+                    in = c0 * 256u + cb;
                 }
+                const uint32_t c = in >> 8;
+                const uint32_t addc = in & 1u;
+                const uint32_t hpc = (in >> 1) & 1u;
+                const uint32_t hnc = (in >> 2) & 1u;
                 const uint64_t eq = qbk.eq(c);
                 const uint64_t xh = eq | vn;
-                const uint64_t xhvp = xh & vp;
-                const uint64_t s1 = vp + xhvp;
-                const uint64_t c1 = s1 < vp ? 1ull : 0ull;
-                const uint64_t s2 = s1 + addc;
-                const uint64_t c2 = s2 < s1 ? 1ull : 0ull;
-                const uint32_t add_out = static_cast<uint32_t>(c1 | c2);
-                uint64_t d0 = (s2 ^ vp) | xh;
-                uint64_t hn = vp & d0;
-                uint64_t hp = vn | ~(vp | d0);
-                d0 &= bmask;
-                hn &= bmask;
-                hp &= bmask;
+                uint32_t add_out;
+                const uint64_t s2 = add_carry64(vp, xh & vp, addc, &add_out);
+                const uint64_t d0 = (s2 ^ vp) | xh;
+                const uint64_t hn = vp & d0;
+                const uint64_t hp = vn | ~(vp | d0);
                 const uint32_t hp_out = static_cast<uint32_t>(hp >> 63);
                 const uint32_t hn_out = static_cast<uint32_t>(hn >> 63);
                 const uint64_t x = (hp << 1) | hpc;
                 const uint64_t hns = (hn << 1) | hnc;
-                const uint64_t nvn = x & d0;
-                const uint64_t nvp = (hns | ~(d0 | x)) & bmask;
-                vp = nvp;
-                vn = nvn;
-                payload = c | (add_out << 8) | (hp_out << 9) | (hn_out << 10);
-                if (r < R - 1 && gl == G - 1) stripe_buf[j0] = static_cast<uint8_t>(add_out | (hp_out << 1) | (hn_out << 2));
-                // band store of column J = j0 + 1
-                const int blo = band.blo(j0 + 1);
-                const int slotb = blk - blo;
+                vn = x & d0;
+                vp = hns | ~(d0 | x);
+                payload = c * 256u + add_out + hp_out * 2u + hn_out * 4u;
+                if (r < R - 1 && gl == G - 1) stripe_buf[j0] = static_cast<uint8_t>(payload & 7u);
+                // band store of column J = j0 + 1; blo(J) steps by one every 64 columns
+                if (((j0 + 1) - (band.E + 3)) > 0 && (((j0 + 1) - (band.E + 3)) & 63) == 0)
+                    blo_cur = min(blo_cur + 1, nb - band.W);
+                const int slotb = blk - blo_cur;
                 if (slotb >= 0 && slotb < band.W) {
                     uint4* dst = reinterpret_cast<uint4*>(recs + (static_cast<uint64_t>(j0) * band.W + slotb) * kRecBytes);
-                    dst[0] = make_uint4(static_cast<uint32_t>(vp), static_cast<uint32_t>(vp >> 32),
-                                        static_cast<uint32_t>(vn), static_cast<uint32_t>(vn >> 32));
-                    dst[1] = make_uint4(static_cast<uint32_t>(hp), static_cast<uint32_t>(hp >> 32),
-                                        static_cast<uint32_t>(hn), static_cast<uint32_t>(hn >> 32));
+                    *dst = make_uint4(static_cast<uint32_t>(vp), static_cast<uint32_t>(vp >> 32),
+                                      static_cast<uint32_t>(hp), static_cast<uint32_t>(hp >> 32));
                 }
-                if (is_last) {
-                    if ((hp >> score_bit) & 1) score += 1;
-                    if ((hn >> score_bit) & 1) score = score > 0 ? score - 1 : 0;
+                // fitting: score of the last block's bit m-1 per column (other lanes have
+                // smask = 0); global mode reads the distance off the final column instead
+                if (any_fit && !stopped) {
+                    const int sc = score + ((hp & smask) ? 1 : 0) - ((hn & smask) ? 1 : 0);
+                    score = sc > 0 ? sc : 0;
                     if (score < best) {
                         best = score;
                         best_col = j0 + 1;
                     }
-                    if (fitting && score > best + margin) {
-                        stopped = true;
-                        ncols = j0 + 1;
-                    }
+                    if (fitting && smask && score > best + margin) stopped = true;
                 }
             }
-            // the group's last lane owns the score; everyone stops when it abandons
-            const uint32_t sv = __shfl_sync(PHR_FULL_MASK, stopped ? 1u : 0u, last_lane, G);
-            if (fitting && r == R - 1) stop_r = sv != 0;
+            if (any_fit && (s & 15) == 15) {
+                // the group's last lane owns the score; all stop once it abandoned
+                const uint32_t sv = __shfl_sync(PHR_FULL_MASK, stopped ? 1u : 0u, last_lane, G);
+                if (fitting && r == R - 1) stop_r = sv != 0;
+            }
+        }
+        if (blk_act) {
+            const uint64_t rows = (blk == nb - 1 && (m & 63)) ? ((1ull << (m & 63)) - 1) : ~0ull;
+            colsum += __popcll(vp & rows) - __popcll(vn & rows);
         }
         __syncwarp();
     }
-    (void)ncols;
+    // D[m][n] = D[0][n] + sum of the vertical deltas of column n = n + sum(VP) - sum(VN)
+    for (int o = 1; o < G; o <<= 1) colsum += __shfl_xor_sync(PHR_FULL_MASK, colsum, o, G);
+    if (!fitting) score = n + colsum;
 
-    // broadcast results from the lane owning the last block
+    // results of each group, from the lane owning the last block
     const int ed_all = __shfl_sync(PHR_FULL_MASK, fitting ? best : score, last_lane, G);
     const int end_all = __shfl_sync(PHR_FULL_MASK, fitting ? best_col : n, last_lane, G);
     const bool band_ok = ed_all <= band.E;
@@ -271,86 +290,106 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
         atomicMax(P.redo_need_max, static_cast<unsigned long long>(need_full));
     }
 
-    // ---- traceback: group-cooperative bit walk ---------------------------------
+    // ---- traceback: every group walks its own pair, all groups in lockstep ----------
+    // Window: group lane L holds column jw - L (G columns) and query blocks bw, bw+1 (128
+    // rows). Each iteration classifies the current cell and consumes the whole run of
+    // that move type: a D run from the column's VP bits, an I run from a ballot over the
+    // row's VP/HP bits, an M or X run from a ballot along the diagonal.
+    const int gbase = lane & ~(G - 1);
+    const unsigned gmask = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
     RunWriter rw;
     rw.init(runs, static_cast<uint32_t>(m + n + 2), gl == 0);
-    int i = trace ? m : 0;
-    int j = trace ? end_all : 0;
-    // window: lane gl holds column (jw - gl), blocks bw (lo) and bw+1 (hi) of that column
-    int jw = -1, bw = -1;
-    uint64_t lo_vp = 0, lo_vn = 0, lo_hp = 0, lo_hn = 0, hi_vp = 0, hi_vn = 0, hi_hp = 0, hi_hn = 0;
+    int i = trace ? m : 0, j = trace ? end_all : 0;
+    int jw = -1, bw = -2;
+    uint64_t lvp = 0, lhp = 0, hvp = 0, hhp = 0;
     for (;;) {
         const bool want = trace && i > 0 && j > 0;
         if (!__any_sync(PHR_FULL_MASK, want)) break;
-        // (re)load the window when the current cell is outside it
-        const int r1 = i - 1;  // query row bit of cell (i, j)
-        const bool need_load =
-            want && (jw < 0 || j > jw || j <= jw - G || (r1 >> 6) > bw + 1 || r1 < 64 * bw + 1);
-        if (__any_sync(PHR_FULL_MASK, need_load)) {
-            if (need_load) {
-                jw = j;
-                const int bhi = r1 >> 6;
-                bw = bhi - 1;  // may be -1: then the lo block is absent
-                const int col = jw - gl;
-                lo_vp = lo_vn = lo_hp = lo_hn = hi_vp = hi_vn = hi_hp = hi_hn = 0;
-                if (col >= 1) {
-                    const int blo = band.blo(col);
-                    const uint8_t* base = recs + static_cast<uint64_t>(col - 1) * band.W * kRecBytes;
-                    const int sh = bhi - blo;
-                    if (sh >= 0 && sh < band.W) {
-                        const uint4 a = reinterpret_cast<const uint4*>(base + sh * kRecBytes)[0];
-                        const uint4 b = reinterpret_cast<const uint4*>(base + sh * kRecBytes)[1];
-                        hi_vp = a.x | (static_cast<uint64_t>(a.y) << 32);
-                        hi_vn = a.z | (static_cast<uint64_t>(a.w) << 32);
-                        hi_hp = b.x | (static_cast<uint64_t>(b.y) << 32);
-                        hi_hn = b.z | (static_cast<uint64_t>(b.w) << 32);
-                    }
-                    const int sl = bw - blo;
-                    if (bw >= 0 && sl >= 0 && sl < band.W) {
-                        const uint4 a = reinterpret_cast<const uint4*>(base + sl * kRecBytes)[0];
-                        const uint4 b = reinterpret_cast<const uint4*>(base + sl * kRecBytes)[1];
-                        lo_vp = a.x | (static_cast<uint64_t>(a.y) << 32);
-                        lo_vn = a.z | (static_cast<uint64_t>(a.w) << 32);
-                        lo_hp = b.x | (static_cast<uint64_t>(b.y) << 32);
-                        lo_hn = b.z | (static_cast<uint64_t>(b.w) << 32);
-                    }
+        const int r1 = i - 1;
+        const bool reload = want && (jw < 0 || j <= jw - G || (r1 >> 6) > bw + 1 || r1 < 64 * bw);
+        if (reload) {
+            jw = j;
+            bw = (r1 >> 6) - 1;
+            const int col = jw - gl;
+            lvp = lhp = hvp = hhp = 0;
+            if (col >= 1) {
+                const int blo = band.blo(col);
+                const uint8_t* base = recs + static_cast<uint64_t>(col - 1) * band.W * kRecBytes;
+                const int sh = bw + 1 - blo;
+                if (sh >= 0 && sh < band.W) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(base + sh * kRecBytes);
+                    hvp = a.x | (static_cast<uint64_t>(a.y) << 32);
+                    hhp = a.z | (static_cast<uint64_t>(a.w) << 32);
+                }
+                const int sl = bw - blo;
+                if (bw >= 0 && sl >= 0 && sl < band.W) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(base + sl * kRecBytes);
+                    lvp = a.x | (static_cast<uint64_t>(a.y) << 32);
+                    lhp = a.z | (static_cast<uint64_t>(a.w) << 32);
                 }
             }
         }
-        // every lane extracts the decision bits of row r1 (and r1-1) for its own column
-        uint32_t bits = 0;
+        const int src = want ? jw - j : 0;   // group lane holding the current column
+        const int base_row = 64 * bw;        // window row 0 (may be -64)
+        const int dlt = gl - src;            // diagonal offset of this lane's cell
+        const int col = jw - gl;
+        const int p1 = r1 - base_row;        // current row in the window, 0..127
+        uint32_t vp1 = 0, hp1 = 0, dcode = 3;
+        bool isI = false;
+        int drun = 1;
         if (want) {
-            const int b1 = r1 >> 6, o1 = r1 & 63;
-            const uint64_t vpw = (b1 == bw + 1) ? hi_vp : lo_vp;
-            const uint64_t vnw = (b1 == bw + 1) ? hi_vn : lo_vn;
-            const uint64_t hpw = (b1 == bw + 1) ? hi_hp : lo_hp;
-            bits |= static_cast<uint32_t>((vpw >> o1) & 1);
-            bits |= static_cast<uint32_t>((hpw >> o1) & 1) << 1;
-            bits |= static_cast<uint32_t>((vnw >> o1) & 1) << 2;
-            if (r1 >= 1) {
-                const int r0 = r1 - 1;
-                const int b0 = r0 >> 6, o0 = r0 & 63;
-                const uint64_t hp0 = (b0 == bw + 1) ? hi_hp : lo_hp;
-                const uint64_t hn0 = (b0 == bw + 1) ? hi_hn : lo_hn;
-                bits |= static_cast<uint32_t>((hp0 >> o0) & 1) << 3;
-                bits |= static_cast<uint32_t>((hn0 >> o0) & 1) << 4;
+            vp1 = bit128(lvp, hvp, p1);
+            hp1 = bit128(lhp, hhp, p1);
+            isI = dlt >= 0 && col >= 1 && !vp1 && hp1;
+            // this lane's cell on the current diagonal: 0 M, 1 X, 2 not diagonal, 3 invalid
+            const int rd = r1 - dlt;
+            const int pd = rd - base_row;
+            if (dlt >= 0 && col >= 1 && rd >= 0 && pd >= 0) {
+                if (bit128(lvp, hvp, pd) | bit128(lhp, hhp, pd)) {
+                    dcode = 2;
+                } else {  // diagonal: M when query byte rd equals target byte col-1
+                    dcode = sym_at<S>(qb, rd) == sym_at<S>(tb, col - 1) ? 0u : 1u;
+                }
             }
+            // D run down this lane's column from row r1 (consecutive VP bits, downward)
+            const int p = p1;
+            const uint64_t hi = p >= 64 ? (p == 127 ? hvp : ((hvp << (127 - p)) | (lvp >> (p - 63)))) : (lvp << (63 - p));
+            const uint64_t lo = p >= 64 ? (lvp << (127 - p)) : 0ull;
+            drun = ~hi ? __clzll(~hi) : 64 + (~lo ? __clzll(~lo) : 64);
+            drun = min(drun, p + 1);
         }
-        const int src = want ? (jw - j) : gl;
-        const uint32_t cb = __shfl_sync(PHR_FULL_MASK, bits, src, G);
+        const int src_lane = gbase + src;
+        const uint32_t cur = __shfl_sync(PHR_FULL_MASK, vp1 | (hp1 << 1) | (dcode << 2), src_lane);
+        const int drun_src = __shfl_sync(PHR_FULL_MASK, drun, src_lane);
+        const unsigned mI = (__ballot_sync(PHR_FULL_MASK, isI) >> gbase) & gmask;
+        const unsigned mM = (__ballot_sync(PHR_FULL_MASK, dcode == 0) >> gbase) & gmask;
+        const unsigned mX = (__ballot_sync(PHR_FULL_MASK, dcode == 1) >> gbase) & gmask;
         if (want) {
-            if (cb & 1) {
-                rw.push(3, 1);  // D: query-extra
-                --i;
-            } else if (cb & 2) {
-                rw.push(2, 1);  // I: target-extra
-                --j;
+            int op, run;
+            if (cur & 1u) {
+                op = 3;  // D: query-extra
+                run = drun_src;
             } else {
-                const int dh = (r1 >= 1) ? static_cast<int>((cb >> 3) & 1) - static_cast<int>((cb >> 4) & 1) : 1;
-                const int cost = dh - static_cast<int>((cb >> 2) & 1);
-                rw.push(cost == 0 ? 0 : 1, 1);
-                --i;
-                --j;
+                unsigned sh;
+                if (cur & 2u) {
+                    op = 2;  // I: target-extra
+                    sh = mI >> src;
+                } else {
+                    op = ((cur >> 2) & 3u) == 0 ? 0 : 1;
+                    sh = (op == 0 ? mM : mX) >> src;
+                }
+                run = (~sh) ? __ffs(~sh) - 1 : 32 - src;
+                run = min(run, G - src);
+            }
+            run = max(run, 1);
+            rw.push(static_cast<uint32_t>(op), static_cast<uint32_t>(run));
+            if (op == 3) {
+                i -= run;
+            } else if (op == 2) {
+                j -= run;
+            } else {
+                i -= run;
+                j -= run;
             }
         }
     }
@@ -360,41 +399,33 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
         rw.flush();
     }
     __syncwarp();
-    // every group lane tracked the same runs; lane 0's writes are the ones that landed
+    // every group lane tracked the same runs; the group leader stored them
     const uint32_t nr = rw.n;
     const bool fmt = trace && !rw.overflow;
+    const uint32_t nr_fmt = fmt ? nr : 0;
+    const uint32_t nrmax = __reduce_max_sync(PHR_FULL_MASK, nr_fmt);
+    const uint32_t rounds = (nrmax + G - 1) / G;
+    char* out = act ? P.text + P.text_off[pid] : nullptr;
     uint32_t tl = 0;
-    {
-        const uint32_t nr_fmt = fmt ? nr : 0;
-        const uint32_t nrmax = __reduce_max_sync(PHR_FULL_MASK, nr_fmt);
-        (void)nrmax;
-        // groups format independently; format_runs_group loops to the group's own count,
-        // so keep every lane of the warp in the same loop by iterating to the warp max
-        const int l = gl;
-        uint32_t base = 0;
-        const uint32_t rounds = (nrmax + G - 1) / G;
-        char* out = act ? P.text + P.text_off[pid] : nullptr;
-        for (uint32_t rr = 0; rr < rounds; ++rr) {
-            const uint32_t c = rr * G + l;
-            uint32_t len = 0, run = 0;
-            if (c < nr_fmt) {
-                run = runs[nr_fmt - 1 - c];
-                len = ndigits(run >> 2) + 1;
-            }
-            const uint32_t incl = group_incl_scan(len, G);
-            if (c < nr_fmt) {
-                char* p = out + base + incl - len;
-                uint32_t v = run >> 2;
-                const uint32_t nd = len - 1;
-                for (int dd = static_cast<int>(nd) - 1; dd >= 0; --dd) {
-                    p[dd] = static_cast<char>('0' + v % 10);
-                    v /= 10;
-                }
-                p[nd] = op_char(run & 3);
-            }
-            base += __shfl_sync(PHR_FULL_MASK, incl, G - 1, G);
+    for (uint32_t rr = 0; rr < rounds; ++rr) {
+        const uint32_t c = rr * G + gl;
+        uint32_t len = 0, run = 0;
+        if (c < nr_fmt) {
+            run = runs[nr_fmt - 1 - c];
+            len = ndigits(run >> 2) + 1;
         }
-        tl = base;
+        const uint32_t incl = group_incl_scan(len, G);
+        if (c < nr_fmt) {
+            char* pp = out + tl + incl - len;
+            uint32_t v = run >> 2;
+            const uint32_t nd = len - 1;
+            for (int dd = static_cast<int>(nd) - 1; dd >= 0; --dd) {
+                pp[dd] = static_cast<char>('0' + v % 10);
+                v /= 10;
+            }
+            pp[nd] = op_char(run & 3);
+        }
+        tl += __shfl_sync(PHR_FULL_MASK, incl, G - 1, G);
     }
     if (fmt && gl == 0) {
         PairOut o;
