@@ -343,3 +343,74 @@ Engine.align_packed = lambda self, index, packed, strategy=A.BALANCED, gap_model
     self, index, packed, strategy, gap_model)
 Engine.sketch = lambda self, seqs, k=21, w=11, alphabet=A.ALPHABET_DNA: _sketch(self, seqs, k, w, alphabet)
 Engine.seed_chain = lambda self, index, sketches: _seed_chain(self, index, sketches)
+
+
+# ---------------------------------------------------------------------------
+# Serving loop (phr_server_*)
+# ---------------------------------------------------------------------------
+class Server:
+    """Continuous-batching read server over a device-resident index."""
+
+    def __init__(self, engine, index, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, max_batch_reads=4096,
+                 max_batch_bases=0, max_wait_us=200, n_streams=2, hbm_reserve_bytes=0):
+        self._eng = engine
+        self._lib = engine._lib
+        self._index = index
+        cfg = A.ServerConfig(A.AlignConfig(strategy, gap_model), max_batch_reads, max_batch_bases, hbm_reserve_bytes,
+                             max_wait_us, n_streams)
+        h = C.c_void_p()
+        engine.check(self._lib.phr_server_create(engine.handle, index.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        K = 1 if strategy == A.FAST else 2 if strategy == A.BALANCED else 50
+        self._K = K
+
+    def submit(self, read):
+        rid = C.c_uint64()
+        read = bytes(read)
+        st = self._lib.phr_server_submit(self._h, read, len(read), C.byref(rid))
+        if st != A.PHR_OK:
+            raise EngineError(st, "phr_server_submit failed")
+        return rid.value
+
+    def poll(self, max_results=4096, wait_us=0, max_read_len=100000):
+        res = (A.ServerResult * max_results)()
+        acap = max_results * 2 * self._K + 16
+        aln = np.zeros(acap, dtype=ALN_DTYPE)
+        ccap = acap * (6 * 1024 + 16)
+        cig = np.zeros(ccap, dtype=np.uint8)
+        n = C.c_uint32()
+        st = self._lib.phr_server_poll(self._h, res, max_results, aln.ctypes.data, acap, cig.ctypes.data, ccap,
+                                       wait_us, C.byref(n))
+        if st not in (A.PHR_OK,):
+            raise EngineError(st, "phr_server_poll failed")
+        out = []
+        cb = cig.tobytes()
+        k = 0
+        for i in range(n.value):
+            r = res[i]
+            alns = []
+            for _ in range(r.n_aln):
+                a = aln[k]
+                k += 1
+                alns.append((cb[a["cigar_off"]:a["cigar_off"] + a["cigar_len"]].decode(), int(a["edit_distance"]),
+                             int(a["query_start"]), int(a["query_end"]), int(a["target_start"]),
+                             int(a["target_end"])))
+            out.append((int(r.request_id), (int(r.outcome), int(r.has_result), int(r.reverse), alns),
+                        float(r.latency_us)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            st = self._lib.phr_server_destroy(self._h)
+            self._h = None
+            if st != A.PHR_OK:
+                raise EngineError(st, "server stopped with an error")
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+Engine.server = lambda self, index, **kw: Server(self, index, **kw)
