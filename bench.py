@@ -171,14 +171,18 @@ def run_engine(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     n_a, n_b = args.n_a, args.n_b
+    from phraya_b200 import datagen as D
     t_gen = time.perf_counter()
-    set_a, set_b = make_workload(n_a, n_b, seed=rank)
+    dev_a = D.extension_pairs_device(n_a, 100, 300, 0.05, seed=2 * rank, device=f"cuda:{dev}")
+    dev_b = D.extension_pairs_device(n_b, 64, 2048, 0.05, seed=2 * rank + 1, log_uniform=True, device=f"cuda:{dev}")
+    set_a, set_b = D.to_packed(dev_a), D.to_packed(dev_b)
+    torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
     eng = P.Engine(dev)
     L = eng._lib
     stream = torch.cuda.ExternalStream(L.phr_ctx_stream(eng.handle), device=dev)
 
-    # ---- device-resident copies (value) --------------------------------------
+    # ---- device-resident batches (value) -------------------------------------
     def to_dev(p):
         d = {k: torch.from_numpy(np.ascontiguousarray(getattr(p, k))).to(f"cuda:{dev}")
              for k in ("seq", "q_off", "q_len", "t_off", "t_len")}
@@ -293,27 +297,29 @@ def run_engine(args, rank, world):
 
     if rank != 0:
         return
-    # ---- roofline of the dominant kernel --------------------------------------
+    # ---- roofline of the dominant kernel (its device time per step, CUDA events) ----
     peaks, peak_src = load_peaks()
     name, (nl, tot) = max(ktimes.items(), key=lambda kv: kv[1][1])
-    per_launch_ms = tot / nl
-    sm_clock = (clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0))
+    step_ms = tot / args.steps           # all launches of that kernel in one step
     int_peak_tops = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     if name.startswith("myers"):
-        ops = dp_cells(set_b) * 22.0 / 32.0      # per launch: one Myers pass over set B
-        achieved = ops / (per_launch_ms / 1000.0) / 1e12
-        roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tops/s",
-                "frac": achieved / int_peak_tops, "traffic": None, "kernel": name,
-                "work": "sum(m*n) * 22/32 integer ops per launch (set B)",
-                "peak_source": "nominal issue rate 148 SMs x 4 x 32 lanes x max SM clock (no measured int peak)"}
-    else:
-        # WFA: DP-equivalent cells of set A per launch against the same issue peak
+        ops = dp_cells(set_b) * 22.0 / 32.0
+        work = "sum(m*n) * 22/32 integer ops per step (set B, all launches incl. band redo)"
+    elif name.startswith("wfa_affine"):
         ops = dp_cells(set_a)
-        achieved = ops / (per_launch_ms / 1000.0) / 1e12
-        roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tcells/s",
-                "frac": achieved / int_peak_tops, "traffic": None, "kernel": name,
-                "work": "DP-equivalent cells of set A per launch",
-                "peak_source": "nominal issue rate (no measured int peak)"}
+        work = "DP-equivalent cells of set A per step"
+    else:
+        ops = dp_cells(set_a)
+        work = "DP-equivalent cells of set A per step"
+    achieved = ops / (step_ms / 1000.0) / 1e12
+    roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tops/s",
+            "frac": achieved / int_peak_tops, "traffic": args.traffic_gb_per_step, "kernel": name,
+            "kernel_ms_per_step": step_ms, "launches_per_step": nl / args.steps, "work": work,
+            "peak_source": "nominal integer issue rate 148 SMs x 4 x 32 lanes x max SM clock "
+                           f"({peaks.get('sm_max_mhz', 1965.0)} MHz, {peak_src}); no measured integer peak exists"}
+    pipe = None
+    if not args.no_pipeline:
+        pipe = run_pipeline(eng, dev, args)
     cpu = cpu_baseline(set_a, set_b, n_a, n_b, os.cpu_count() or 1) if not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -330,8 +336,90 @@ def run_engine(args, rank, world):
             "kernel_ms": {k: round(v[1] / args.steps, 3) for k, v in ktimes.items()},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "pipeline": pipe,
             "datagen_s": round(t_gen, 1)}
     print(json.dumps(line))
+
+
+def run_pipeline(eng, dev, args):
+    """Read-pipeline figures: align_read over a 1 Mbp reference (20,000 x 150 bp reads, 1 %
+    substitutions + 0.05 % 1-3 bp indels, both strands): batched vs one read per call,
+    and a served mixed Poisson stream (90 % 150 bp at 1 % error, 10 % long reads with
+    lognormal lengths, median 8 kb, 5 % error) with p50/p99 latency of the short reads."""
+    import ctypes as C
+    import numpy as np
+    from phraya_b200 import _abi as A
+    from phraya_b200 import datagen as D
+    from phraya_b200.batch import PackedReads
+
+    out = {}
+    ref = D.random_reference(1_000_000, seed=100)
+    idx = eng.index(ref)
+    packed, _, _ = D.reads_on_reference(ref, args.reads, 150, 0.0105, seed=101, sub_frac=0.952, max_indel=3)
+    reads = [bytes(packed.seq[o:o + l]) for o, l in zip(packed.off, packed.len)]
+    for strat, name in ((A.BALANCED, "balanced"), (A.SENSITIVE, "sensitive_affine")):
+        eng.align_packed(idx, packed, strat, A.GAP_AFFINE)  # warm-up
+        t0 = time.perf_counter()
+        rr, aln, cig, st = eng.align_packed(idx, packed, strat, A.GAP_AFFINE)
+        dt = time.perf_counter() - t0
+        out[f"batched_{name}_reads_per_s"] = len(reads) / dt
+        out[f"batched_{name}_placed_frac"] = st[0] / len(reads)
+    # one read per call (the reference API's shape), on a sample
+    k = min(300, len(reads))
+    one = [PackedReads([r]) for r in reads[:k]]
+    eng.align_packed(idx, one[0], A.BALANCED, A.GAP_AFFINE)
+    t0 = time.perf_counter()
+    for pr in one:
+        eng.align_packed(idx, pr, A.BALANCED, A.GAP_AFFINE)
+    out["percall_balanced_reads_per_s"] = k / (time.perf_counter() - t0)
+    out["batched_over_percall"] = out["batched_balanced_reads_per_s"] / out["percall_balanced_reads_per_s"]
+    # served mixed stream
+    rng = np.random.default_rng(102)
+    n_req = args.reads
+    n_long = n_req // 10
+    longp, _, _ = D.reads_on_reference(
+        ref, n_long, error=0.05, seed=103, sub_frac=0.4, max_indel=3,
+        length_sampler=lambda g, n: np.clip(np.exp(g.normal(np.log(8000), 0.5, n)), 1000, 50000).astype(np.int64))
+    longs = [bytes(longp.seq[o:o + l]) for o, l in zip(longp.off, longp.len)]
+    stream = reads[:n_req - n_long] + longs
+    order = rng.permutation(len(stream))
+    stream = [stream[i] for i in order]
+    is_short = [len(r) <= 500 for r in stream]
+    gaps = rng.exponential(1.0 / args.served_rate, len(stream))
+    srv = eng.server(idx, strategy=A.BALANCED, max_batch_reads=2048, max_wait_us=1000, n_streams=3)
+    # warm the workers
+    for r in stream[:64]:
+        srv.submit(r)
+    got = 0
+    while got < 64:
+        got += len(srv.poll(4096, wait_us=20000))
+    lat = {}
+    ids = {}
+    t_start = time.perf_counter()
+    next_t = t_start
+    i = 0
+    done = 0
+    while done < len(stream):
+        now = time.perf_counter()
+        while i < len(stream) and next_t <= now:
+            ids[srv.submit(stream[i])] = i
+            next_t += gaps[i]
+            i += 1
+        for rid, res, l in srv.poll(4096, wait_us=200 if i >= len(stream) else 0):
+            lat[ids[rid]] = l
+            done += 1
+    t_total = time.perf_counter() - t_start
+    srv.close()
+    sl = sorted(lat[j] for j in range(len(stream)) if is_short[j])
+    al = sorted(lat.values())
+    out["served"] = {"rate_offered_reads_per_s": args.served_rate, "reads": len(stream), "long_reads": n_long,
+                     "throughput_reads_per_s": len(stream) / t_total,
+                     "p50_ms_150bp": sl[len(sl) // 2] / 1000.0, "p99_ms_150bp": sl[int(len(sl) * 0.99)] / 1000.0,
+                     "p99_ms_all": al[int(len(al) * 0.99)] / 1000.0}
+    out["served_over_percall"] = out["served"]["throughput_reads_per_s"] / out["percall_balanced_reads_per_s"]
+    out["workload"] = ("align_read, 1 Mbp i.i.d. reference, 150 bp reads both strands, 1 % subs + 0.05 % "
+                       "1-3 bp indels; served: Poisson arrivals, 90 % 150 bp + 10 % lognormal long reads")
+    return out
 
 
 def main():
@@ -343,6 +431,11 @@ def main():
     ap.add_argument("--n-a", type=int, default=N_A_DEFAULT)
     ap.add_argument("--n-b", type=int, default=N_B_DEFAULT)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-pipeline", action="store_true", help="skip the read-pipeline / serving section")
+    ap.add_argument("--reads", type=int, default=20000, help="reads of the read-pipeline section")
+    ap.add_argument("--served-rate", type=float, default=100000.0, help="Poisson arrival rate (reads/s)")
+    ap.add_argument("--traffic-gb-per-step", type=float, default=None,
+                    help="DRAM bytes per step of the dominant kernel from an ncu capture (reported as is)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

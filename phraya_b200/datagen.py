@@ -130,3 +130,63 @@ def reads_on_reference(reference, n, length=150, error=0.01, seed=1, sub_frac=0.
             r = COMP[r[::-1]]
         reads.append(r.tobytes())
     return PackedReads(reads), starts, rev
+
+
+def extension_pairs_device(n, lo=100, hi=300, max_div=0.05, seed=0, log_uniform=False, max_indel=5, device="cuda"):
+    """`extension_pairs` generated on the GPU with torch (same model, its own RNG
+    stream): returns a dict of device tensors seq, q_off, q_len, t_off, t_len."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    if log_uniform:
+        u = torch.rand(n, generator=g, device=device, dtype=torch.float64)
+        qlen = torch.exp(np.log(lo) + u * (np.log(hi) - np.log(lo))).long()
+    else:
+        qlen = torch.randint(lo, hi + 1, (n,), generator=g, device=device)
+    qlen = qlen.clamp(lo, hi)
+    div = torch.rand(n, generator=g, device=device, dtype=torch.float64) * max_div
+    q_start = torch.zeros(n, dtype=torch.long, device=device)
+    q_start[1:] = torch.cumsum(qlen, 0)[:-1]
+    nq = int(qlen.sum().item())
+    q = torch.randint(0, 4, (nq,), generator=g, device=device, dtype=torch.uint8)
+    # mutation (see _mutate)
+    pair_of = torch.repeat_interleave(torch.arange(n, device=device), qlen)
+    ev = torch.rand(nq, generator=g, device=device, dtype=torch.float64) < div[pair_of]
+    kind = torch.rand(nq, generator=g, device=device)
+    is_sub = ev & (kind < 0.7)
+    is_ins = ev & (kind >= 0.7) & (kind < 0.85)
+    is_del = ev & (kind >= 0.85)
+    klen = torch.randint(1, max_indel + 1, (nq,), generator=g, device=device)
+    pos = torch.arange(nq, device=device)
+    seg_end = (q_start + qlen)[pair_of]
+    del_end = torch.where(is_del, torch.minimum(pos + klen, seg_end), torch.zeros_like(pos))
+    run = torch.cummax(del_end, 0).values
+    keep = ~(run > pos)
+    ins_len = torch.where(is_ins & keep, klen, torch.zeros_like(klen))
+    per = keep.long() + ins_len
+    out_off = torch.zeros(nq + 1, dtype=torch.long, device=device)
+    out_off[1:] = torch.cumsum(per, 0)
+    nt = int(out_off[-1].item())
+    t = torch.randint(0, 4, (nt,), generator=g, device=device, dtype=torch.uint8)
+    shift = torch.randint(1, 4, (nq,), generator=g, device=device, dtype=torch.uint8)
+    kept = torch.where(is_sub, (q + shift) % 4, q)
+    t[out_off[:-1][keep]] = kept[keep]
+    ends = torch.cumsum(qlen, 0)
+    tlen = out_off[ends] - out_off[q_start]
+    t_start = torch.zeros(n, dtype=torch.long, device=device)
+    t_start[1:] = torch.cumsum(tlen, 0)[:-1]
+    qo = q_start + t_start
+    to = qo + qlen
+    bases = torch.tensor(list(b"ACGT"), dtype=torch.uint8, device=device)
+    seq = torch.empty(nq + nt + 64, dtype=torch.uint8, device=device)
+    seq[torch.repeat_interleave(qo - q_start, qlen) + torch.arange(nq, device=device)] = bases[q.long()]
+    seq[torch.repeat_interleave(to - t_start, tlen) + torch.arange(nt, device=device)] = bases[t.long()]
+    return {"seq": seq, "q_off": qo.to(torch.uint64), "q_len": qlen.to(torch.uint32),
+            "t_off": to.to(torch.uint64), "t_len": tlen.to(torch.uint32), "n": n, "seq_bytes": nq + nt}
+
+
+def to_packed(d):
+    """Host PackedPairs copy of a device pair dict."""
+    return PackedPairs.from_arrays(d["seq"][:d["seq_bytes"]].cpu().numpy(), d["q_off"].cpu().numpy(),
+                                   d["q_len"].cpu().numpy(), d["t_off"].cpu().numpy(), d["t_len"].cpu().numpy())
