@@ -109,7 +109,7 @@ typedef struct {
 typedef struct phr_ctx phr_ctx;
 
 typedef struct {
-    uint64_t workspace_bytes;  /* device scratch reserved up front; 0 = default (1 GiB) */
+    uint64_t workspace_bytes;  /* cap on extension scratch; 0 = default (8 GiB)         */
     int32_t tune_file_enable;  /* 1 = read/write autotuner cache file                   */
     const char* tune_file;     /* NULL = "phraya_b200_tune.txt" in the working dir      */
 } phr_config;
@@ -120,6 +120,20 @@ const char* phr_status_string(phr_status s);
 
 phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out);
 void phr_ctx_destroy(phr_ctx* ctx);
+/* Launch parameters of the extension kernels. No counterpart in the reference (its
+ * kernels are CPU code with nothing to tune); results never depend on them. Keys:
+ *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen 1024
+ *                                        (power of two, 1..32)
+ *   "myers_band_base"                    Myers stored-band half-width base (>= 0)
+ *   "block_threads"                      threads per block of the warp-per-pair kernels
+ *                                        (32..256, multiple of 32)
+ *   "wfa_big_min"                        linear WFA pairs with qlen+tlen >= this run one
+ *                                        per CTA (0 = never)
+ *   "wfa_big_smem"                       shared memory of that kernel, bytes (16 KiB..200 KiB)
+ * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune
+ * file (written by the autotuner); unknown keys and bad values there are ignored. */
+phr_status phr_ctx_set_tune(phr_ctx* ctx, const char* key, int64_t value);
+phr_status phr_ctx_get_tune(const phr_ctx* ctx, const char* key, int64_t* value);
 /* Message describing the last non-PHR_OK status returned on this context. */
 const char* phr_ctx_last_error(const phr_ctx* ctx);
 /* Number of the library's own kernel launches issued on this context so far. */

@@ -89,9 +89,9 @@ def lib():
 class Engine:
     """One device context (phr_ctx): a CUDA stream plus its device workspace."""
 
-    def __init__(self, device=0, workspace_bytes=0):
+    def __init__(self, device=0, workspace_bytes=0, tune_file=None):
         L = lib()
-        cfg = A.Config(workspace_bytes, 0, None)
+        cfg = A.Config(workspace_bytes, 1 if tune_file else 0, tune_file.encode() if tune_file else None)
         h = C.c_void_p()
         st = L.phr_ctx_create(device, C.byref(cfg), C.byref(h))
         if st != A.PHR_OK:
@@ -121,6 +121,15 @@ class Engine:
     def check(self, st):
         if st != A.PHR_OK:
             raise EngineError(st, self._lib.phr_ctx_last_error(self._h).decode())
+
+    def set_tune(self, key, value):
+        """Sets one kernel launch parameter (phr_ctx_set_tune); results never depend on it."""
+        self.check(self._lib.phr_ctx_set_tune(self._h, key.encode(), int(value)))
+
+    def get_tune(self, key):
+        v = C.c_int64()
+        self.check(self._lib.phr_ctx_get_tune(self._h, key.encode(), C.byref(v)))
+        return v.value
 
     @property
     def kernel_launches(self):

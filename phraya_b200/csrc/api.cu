@@ -1,5 +1,6 @@
 // api.cu -- C ABI entry points (include/phraya_gpu.h): context and pairs API.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -136,8 +137,53 @@ phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out) 
     if (cfg && cfg->tune_file_enable) {
         ctx->tune_file_enable = true;
         ctx->tune_file = cfg->tune_file ? cfg->tune_file : "phraya_b200_tune.txt";
+        if (FILE* f = std::fopen(ctx->tune_file.c_str(), "r")) {
+            char key[64];
+            long long v = 0;
+            while (std::fscanf(f, "%63s %lld", key, &v) == 2) phr_ctx_set_tune(c, key, v);
+            std::fclose(f);
+        }
     }
     *out = c;
+    return PHR_OK;
+}
+
+namespace {
+int* tune_field(phr::EngineTune& t, const char* key) {
+    if (!std::strcmp(key, "wfa_group_short")) return &t.wfa_group_short;
+    if (!std::strcmp(key, "wfa_group_long")) return &t.wfa_group_long;
+    if (!std::strcmp(key, "myers_band_base")) return &t.myers_band_base;
+    if (!std::strcmp(key, "block_threads")) return &t.block_threads;
+    if (!std::strcmp(key, "wfa_big_min")) return &t.wfa_big_min;
+    if (!std::strcmp(key, "wfa_big_smem")) return &t.wfa_big_smem;
+    return nullptr;
+}
+bool tune_valid(const char* key, int64_t v) {
+    if (!std::strcmp(key, "wfa_group_short") || !std::strcmp(key, "wfa_group_long"))
+        return v >= 1 && v <= 32 && (v & (v - 1)) == 0;
+    if (!std::strcmp(key, "myers_band_base")) return v >= 0 && v <= (1 << 20);
+    if (!std::strcmp(key, "block_threads")) return v >= 32 && v <= 256 && v % 32 == 0;
+    if (!std::strcmp(key, "wfa_big_min")) return v >= 0 && v <= INT32_MAX;
+    if (!std::strcmp(key, "wfa_big_smem")) return v >= (16 << 10) && v <= (200 << 10) && v % 16 == 0;
+    return false;
+}
+}  // namespace
+
+phr_status phr_ctx_set_tune(phr_ctx* c, const char* key, int64_t value) {
+    if (!c || !key) return PHR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(c->impl.mu);
+    int* f = tune_field(c->impl.tune, key);
+    if (!f) return phr::set_error(&c->impl, PHR_ERR_ARG, std::string("unknown tune key ") + key);
+    if (!tune_valid(key, value)) return phr::set_error(&c->impl, PHR_ERR_ARG, std::string("tune value out of range for ") + key);
+    *f = static_cast<int>(value);
+    return PHR_OK;
+}
+
+phr_status phr_ctx_get_tune(const phr_ctx* c, const char* key, int64_t* value) {
+    if (!c || !key || !value) return PHR_ERR_ARG;
+    int* f = tune_field(const_cast<phr::EngineTune&>(c->impl.tune), key);
+    if (!f) return PHR_ERR_ARG;
+    *value = *f;
     return PHR_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <unordered_set>
 
 #include "engine.cuh"
 
@@ -311,6 +312,8 @@ struct TaskBuild {
     int32_t engine;
     int32_t band_base;
     unsigned long long* need_max;
+    uint64_t* task_need;          // per task
+    unsigned int* need_hist;      // 64 buckets by bit length of the need
 };
 
 __device__ __forceinline__ int key_group(uint32_t k) { return 1 << ((k >> 28) & 7); }
@@ -341,11 +344,6 @@ __device__ __forceinline__ uint64_t myers_need_est(int m, int n, int G, int band
     return need;
 }
 
-__device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool affine) {
-    const uint64_t L = static_cast<uint64_t>(qn + tn);
-    return affine ? (160ull << 10) + 512ull * L : (32ull << 10) + 64ull * L;
-}
-
 __global__ void task_fill_kernel(TaskBuild T) {
     const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (p >= T.n || !T.flag[p]) return;
@@ -369,6 +367,8 @@ __global__ void task_fill_kernel(TaskBuild T) {
     T.task_first[t] = static_cast<uint32_t>(p);
     T.task_count[t] = static_cast<uint8_t>(cnt);
     T.task_group[t] = static_cast<uint8_t>(G);
+    T.task_need[t] = need;
+    atomicAdd(&T.need_hist[64 - __clzll(need | 1)], 1u);
     atomicMax(T.need_max, static_cast<unsigned long long>(need));
     if ((k >> 31) & 1) atomicMin(T.split_min, t);
 }
@@ -385,8 +385,9 @@ __global__ void task_finalize_kernel(TaskBuild T) {
 
 // Redo pass task list: one pair per task, in redo order.
 __global__ void redo_tasks_kernel(const uint32_t* redo_list, const uint32_t* redo_count, const PairDesc* desc,
-                                  int32_t engine, int wfa_g_short, int wfa_g_long, uint32_t* task_first,
-                                  uint8_t* task_count, uint8_t* task_group, uint32_t* ranges) {
+                                  int32_t engine, int wfa_g_short, int wfa_g_long, int32_t big_min,
+                                  uint32_t big_smem, uint32_t* task_first, uint8_t* task_count,
+                                  uint8_t* task_group, uint32_t* ranges) {
     const uint32_t n = *redo_count;
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 0) {
@@ -403,6 +404,7 @@ __global__ void redo_tasks_kernel(const uint32_t* redo_list, const uint32_t* red
     task_first[t] = t;
     task_count[t] = 1;
     task_group[t] = static_cast<uint8_t>(G);
+    if (big_pair(engine, big_min, big_smem, d.qn, d.tn, d.mode)) task_group[t] = kBigTask | 32;
 }
 
 struct FinishParams {
@@ -493,6 +495,7 @@ size_t extend_arena_need(uint64_t n, uint64_t seq_bytes, uint64_t sum_qt) {
     add(n * 6);                           // task count/group
     add(n * 8 * 2);                       // text len + cigar offsets
     add(n * 4);                           // redo list
+    add(n * 8 * 4 + 256);                 // task needs, redo needs, redo task offsets/lengths
     add(64ull << 20);                     // CUB temp
     add(4096);
     return s;
@@ -535,6 +538,11 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     uint8_t* task_group = static_cast<uint8_t*>(take(n));
     uint64_t* tlen = static_cast<uint64_t*>(take(n * 8));
     uint64_t* cigoff = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* task_need = static_cast<uint64_t*>(take(n * 8));
+    unsigned long long* redo_need = static_cast<unsigned long long*>(take(n * 8));
+    uint64_t* rtask_off = static_cast<uint64_t*>(take(n * 8));
+    uint64_t* rtask_len = static_cast<uint64_t*>(take(n * 8));
+    unsigned int* need_hist = static_cast<unsigned int*>(take(64 * 4));
     // counters: [0..3] ranges, [4] split_min, [5] queue head 0, [6] queue head 1,
     // [7] redo count, [8..9] need max (u64), [10] error flag, [12..13] total (u64), [14..17] redo ranges
     uint32_t* cnt = static_cast<uint32_t*>(take(256));
@@ -577,8 +585,9 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     tn_ = t_need;
     cub::DeviceRadixSort::SortPairs(tmp, tn_, keys, keys_s, vals, order, static_cast<int>(n), 0, 32, st);
 
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(need_hist, 0, 64 * 4, st));
     TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, desc,
-                  engine, ctx->tune.myers_band_base, need_max};
+                  engine, ctx->tune.myers_band_base, need_max, task_need, need_hist};
     {
         KernelScope ks(ctx, "task_head");
         task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
@@ -601,11 +610,30 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         task_finalize_kernel<<<1, 1, 0, st>>>(tbp);
     }
 
-    // slot size for the main pass
+    // Main-pass slot: the smallest power of two that covers 99.5 % of the tasks (and no
+    // less than the largest task when that still fits a full grid); tasks needing more
+    // are deferred to the redo passes, which size scratch per task.
     uint64_t h_need = 0;
+    unsigned int h_hist[64];
+    uint32_t h_ranges[4];
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_need, need_max, 8, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_hist, need_hist, sizeof(h_hist), cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_ranges, cnt, sizeof(h_ranges), cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     PHR_CUDA_TRY(ctx, cudaGetLastError());
+    {
+        const uint64_t n_tasks = h_ranges[3];
+        const uint64_t full_grid_warps = static_cast<uint64_t>(ctx->sm_count) * 4 * (ctx->tune.block_threads / 32);
+        if (h_need * full_grid_warps > ctx->scratch_budget && n_tasks > 0) {
+            uint64_t acc = 0, slot = 4096;
+            for (int b = 0; b < 64; ++b) {
+                acc += h_hist[b];
+                slot = b >= 63 ? ~0ull : (1ull << b);
+                if (acc * 1000 >= n_tasks * 995) break;
+            }
+            h_need = std::min(h_need, std::max<uint64_t>(slot, 64 << 10));
+        }
+    }
 
     const bool is_myers = engine == PHR_ENGINE_MYERS_FIT || engine == PHR_ENGINE_MYERS_GLOBAL;
     ExtendParams P{};
@@ -619,21 +647,35 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     P.redo_list = redo_list;
     P.redo_count = cnt + 7;
     P.redo_need_max = need_max;
+    P.redo_need = redo_need;
+    P.task_need = task_need;
     P.engine = engine;
     P.full_band = 0;
     P.band_base = ctx->tune.myers_band_base;
     P.costs = costs;
     P.error_flag = cnt + 10;
+    P.big_min = ctx->tune.wfa_big_min;
+    P.big_smem = static_cast<uint32_t>(ctx->tune.wfa_big_smem);
 
     const int block = ctx->tune.block_threads;
+    // main pass (per_task false): per-warp slots of `slot` bytes; redo passes: per-task
+    // scratch (P.task_off / P.task_len set by the caller, `per_task_total` bytes in all,
+    // `n_tasks_hint` tasks)
     auto launch_pass = [&](const uint32_t* ord, const uint32_t* tfirst, const uint8_t* tcount, const uint8_t* tgroup,
-                           const uint32_t* range0, const uint32_t* range1, uint64_t slot, int full_band) -> phr_status {
-        slot = std::max<uint64_t>((slot + 255) & ~255ull, 4096);
-        // grid: resident blocks per SM, shrunk to the scratch budget
-        uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * 4;
+                           const uint32_t* range0, const uint32_t* range1, uint64_t slot, int full_band,
+                           bool per_task = false, uint64_t per_task_total = 0,
+                           uint64_t n_tasks_hint = 0) -> phr_status {
         const uint64_t warps_per_block = block / 32;
-        while (grid > 1 && grid * warps_per_block * slot > ctx->scratch_budget) grid = (grid + 1) / 2;
-        PHR_CUDA_TRY(ctx, ctx->scratch.reserve(grid * warps_per_block * slot));
+        uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * 4;
+        if (!per_task) {
+            slot = std::max<uint64_t>((slot + 255) & ~255ull, 4096);
+            // grid: resident blocks per SM, shrunk to the scratch budget
+            while (grid > 1 && grid * warps_per_block * slot > ctx->scratch_budget) grid = (grid + 1) / 2;
+            PHR_CUDA_TRY(ctx, ctx->scratch.reserve(grid * warps_per_block * slot));
+        } else {
+            grid = std::max<uint64_t>(1, std::min<uint64_t>(grid, (n_tasks_hint + warps_per_block - 1) / warps_per_block));
+            PHR_CUDA_TRY(ctx, ctx->scratch.reserve(per_task_total));
+        }
         P.scratch = reinterpret_cast<uint8_t*>(ctx->scratch.base);
         P.slot_bytes = slot;
         P.full_band = full_band;
@@ -642,9 +684,13 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         P.tasks.task_count = tcount;
         P.tasks.task_group = tgroup;
         PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 5, 0, 8, st));
-        const char* kname = is_myers ? "myers" : engine == PHR_ENGINE_WFA_LINEAR ? "wfa_linear" : "wfa_affine";
-        const char* kname_b = is_myers ? "myers_bytes" : engine == PHR_ENGINE_WFA_LINEAR ? "wfa_linear_bytes"
-                                                                                       : "wfa_affine_bytes";
+        static const char* const names[2][3][2] = {
+            {{"myers", "myers_bytes"}, {"wfa_linear", "wfa_linear_bytes"}, {"wfa_affine", "wfa_affine_bytes"}},
+            {{"myers_redo", "myers_bytes_redo"}, {"wfa_linear_redo", "wfa_linear_bytes_redo"},
+             {"wfa_affine_redo", "wfa_affine_bytes_redo"}}};
+        const int ek = is_myers ? 0 : engine == PHR_ENGINE_WFA_LINEAR ? 1 : 2;
+        const char* kname = names[per_task][ek][0];
+        const char* kname_b = names[per_task][ek][1];
         P.tasks.range = range0;
         P.queue_head = cnt + 5;
         {
@@ -667,6 +713,17 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             else
                 launch_wfa_affine_bytes(P, static_cast<int>(grid), block, st);
         }
+        if (per_task && engine == PHR_ENGINE_WFA_LINEAR && P.big_min > 0 && n_tasks_hint > 0) {
+            // long pairs of this redo list, one CTA each
+            const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, static_cast<uint64_t>(ctx->sm_count) * 2));
+            PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 24, 0, 8, st));
+            for (int mode = 0; mode < 2; ++mode) {
+                P.tasks.range = mode ? range1 : range0;
+                P.queue_head = cnt + 24 + mode;
+                KernelScope ks(ctx, mode ? "wfa_linear_big_bytes" : "wfa_linear_big");
+                launch_wfa_linear_big(P, big_grid, mode, st);
+            }
+        }
         PHR_CUDA_TRY(ctx, cudaGetLastError());
         return PHR_OK;
     };
@@ -674,35 +731,77 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     phr_status s = launch_pass(order, task_first, task_count, task_group, cnt + 0, cnt + 2, h_need, 0);
     if (s != PHR_OK) return s;
 
-    // overflow redo passes: each pair that did not fit its slot (or, for Myers, whose
-    // edit distance left the stored band) runs again alone with the room it asked for
+    // Redo passes: each pair that did not fit its slot (or, for Myers, whose edit distance
+    // left the stored band) runs again alone, with scratch sized for it: pairs are packed
+    // into passes of at most the workspace budget, one variable-size region per task.
     uint32_t* rlist = redo_list;
     uint32_t* rlist2 = head;  // reuse: free after task build
-    for (int pass = 0; pass < 12; ++pass) {
-        uint32_t h_redo[4] = {0, 0, 0, 0};
-        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_redo, cnt + 7, 4, cudaMemcpyDeviceToHost, st));
-        uint64_t h_need2 = 0;
-        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_need2, need_max, 8, cudaMemcpyDeviceToHost, st));
+    P.task_need = nullptr;
+    std::vector<uint32_t> h_list;
+    std::vector<unsigned long long> h_rneed;
+    std::unordered_set<uint32_t> clamped;
+    for (int round = 0; round < 12; ++round) {
+        uint32_t h_redo = 0;
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_redo, cnt + 7, 4, cudaMemcpyDeviceToHost, st));
         PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
-        if (h_redo[0] == 0) break;
-        if (pass == 11) return set_error(ctx, PHR_ERR_CAPACITY, "extension did not fit after repeated redo passes");
-        if (h_need2 > ctx->scratch_budget)
-            return set_error(ctx, PHR_ERR_OOM, "a single pair needs more scratch than the workspace budget");
-        // tasks from the redo list; swap lists so the pass can append fresh overflows
-        {
-            KernelScope ks(ctx, "redo_tasks");
-            redo_tasks_kernel<<<blocks_for(h_redo[0], T), T, 0, st>>>(rlist, cnt + 7, desc, engine,
-                                                                     ctx->tune.wfa_group_short,
-                                                                     ctx->tune.wfa_group_long, task_first,
-                                                                     task_count, task_group, cnt + 14);
-        }
-        // byte-mode and 2-bit pairs share this list: both launches walk all of it
-        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cnt + 16, cnt + 14, 8, cudaMemcpyDeviceToDevice, st));
+        if (h_redo == 0) break;
+        if (round == 11) return set_error(ctx, PHR_ERR_CAPACITY, "extension did not fit after repeated redo passes");
+        h_list.resize(h_redo);
+        h_rneed.resize(h_redo);
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_list.data(), rlist, h_redo * 4, cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_rneed.data(), redo_need, h_redo * 8, cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
         PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 7, 0, 4, st));
-        P.redo_list = rlist2;
-        s = launch_pass(rlist, task_first, task_count, task_group, cnt + 14, cnt + 16, h_need2, 1);
-        if (s != PHR_OK) return s;
-        std::swap(rlist, rlist2);
+        // largest first, packed into passes within the budget
+        std::vector<uint32_t> idx(h_redo);
+        for (uint32_t i = 0; i < h_redo; ++i) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return h_rneed[a] > h_rneed[b]; });
+        size_t pos = 0;
+        while (pos < idx.size()) {
+            std::vector<uint32_t> pl;
+            std::vector<uint64_t> po, pn;
+            uint64_t tot = 0;
+            while (pos < idx.size()) {
+                uint64_t need = (std::max<uint64_t>(h_rneed[idx[pos]], 4096) + 255) & ~255ull;
+                if (need > ctx->scratch_budget) {
+                    // first-pass needs are estimates: try once with the whole budget
+                    if (clamped.count(h_list[idx[pos]]))
+                        return set_error(ctx, PHR_ERR_OOM, "a single pair needs more scratch than the workspace budget");
+                    clamped.insert(h_list[idx[pos]]);
+                    need = ctx->scratch_budget & ~255ull;
+                }
+                if (!pl.empty() && tot + need > ctx->scratch_budget) break;
+                pl.push_back(h_list[idx[pos]]);
+                po.push_back(tot);
+                pn.push_back(need);
+                tot += need;
+                ++pos;
+            }
+            const uint32_t m = static_cast<uint32_t>(pl.size());
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rlist2, pl.data(), m * 4, cudaMemcpyHostToDevice, st));
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rtask_off, po.data(), m * 8, cudaMemcpyHostToDevice, st));
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rtask_len, pn.data(), m * 8, cudaMemcpyHostToDevice, st));
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cnt + 18, &m, 4, cudaMemcpyHostToDevice, st));
+            {
+                KernelScope ks(ctx, "redo_tasks");
+                redo_tasks_kernel<<<blocks_for(m, T), T, 0, st>>>(rlist2, cnt + 18, desc, engine,
+                                                                 ctx->tune.wfa_group_short, ctx->tune.wfa_group_long,
+                                                                 P.big_min, P.big_smem, task_first, task_count,
+                                                                 task_group, cnt + 14);
+            }
+            // byte-mode and 2-bit pairs share this list: both launches walk all of it
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cnt + 16, cnt + 14, 8, cudaMemcpyDeviceToDevice, st));
+            P.redo_list = rlist;   // fresh overflows of this pass are appended here
+            P.task_off = rtask_off;
+            P.task_len = rtask_len;
+            // synchronise before the scratch buffer may be reallocated for this pass
+            PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+            s = launch_pass(rlist2, task_first, task_count, task_group, cnt + 14, cnt + 16, 0, 1, true, tot, m);
+            P.task_off = nullptr;
+            P.task_len = nullptr;
+            if (s != PHR_OK) return s;
+            PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        }
     }
 
     // pack CIGAR text

@@ -32,6 +32,8 @@ struct EngineTune {
     int wfa_group_long = 32;
     int myers_band_base = 64;
     int block_threads = 256;
+    int wfa_big_min = 4096;          // linear WFA pairs with qn+tn >= this run one per CTA (0: off)
+    int wfa_big_smem = 100 << 10;    // shared memory of that kernel, bytes (two CTAs per SM)
 };
 
 struct Ctx {

@@ -30,15 +30,53 @@ struct ExtendParams {
     uint32_t* redo_list;        // pairs whose scratch need exceeded the slot / band
     uint32_t* redo_count;
     unsigned long long* redo_need_max;
+    unsigned long long* redo_need;   // need of redo_list[k] (same index), may be NULL
+    const uint64_t* task_off;   // when set: task t uses scratch + task_off[t] ...
+    const uint64_t* task_len;   // ... with task_len[t] bytes (redo passes); else per-warp slots
+    const uint64_t* task_need;  // estimated scratch need per task (main pass), may be NULL
     int32_t engine;             // phr_engine
     int32_t full_band;          // Myers: store every block (no band)
     int32_t band_base;          // Myers: band half-width base
     phr_affine_costs costs;
     uint32_t* error_flag;       // set on an internal inconsistency (bounded loops ran out)
+    int32_t big_min;            // linear WFA: pairs with qn+tn >= big_min run one per CTA (0: off)
+    uint32_t big_smem;          // dynamic shared memory of the CTA-per-pair kernel (bytes)
 };
+
+// task_group bit marking a redo task for the CTA-per-pair kernel
+constexpr uint8_t kBigTask = 0x80;
+constexpr int kBigThreads = 512;
+constexpr uint32_t kBigMinFrameCells = 4096;  // smallest shared frame pair worth staging
+
+// Shared-memory words the CTA-per-pair kernel needs for the two sequences of a pair
+// (one extra word each: 32-bit windows read one word past the last symbol).
+__host__ __device__ __forceinline__ uint64_t big_seq_words(int qn, int tn, int mode) {
+    const int per = mode == 0 ? 16 : 4;
+    return static_cast<uint64_t>((qn + per - 1) / per + 1) + static_cast<uint64_t>((tn + per - 1) / per + 1) + 4;
+}
+
+// A linear-WFA pair long enough that one warp would be latency-bound on it, whose
+// sequences fit the CTA's shared memory with room for frames.
+__host__ __device__ __forceinline__ bool big_pair(int32_t engine, int32_t big_min, uint32_t big_smem, int qn, int tn,
+                                                  int mode) {
+    if (big_min <= 0 || engine != PHR_ENGINE_WFA_LINEAR || qn + tn < big_min) return false;
+    return (big_seq_words(qn, tn, mode) + 2ull * kBigMinFrameCells) * 4 <= big_smem;
+}
+
+// First-pass scratch estimate of one WFA pair: room for scores up to 64 + qn/8 (linear:
+// 4 bytes of history per cell plus two value frames; affine: three layers of 8-byte
+// cells). A pair that needs more overflows and is redone with what it asks for.
+__host__ __device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool affine) {
+    const uint64_t L = static_cast<uint64_t>(qn + tn);
+    const uint64_t s = 64 + static_cast<uint64_t>(qn) / 8;
+    if (affine) return (160ull << 10) + 512ull * L;
+    const uint64_t cells = s + 2 * (s * s / 2);
+    return 16 * L + 4 * cells + 4096;
+}
 
 void launch_myers(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st);
+void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
 
 }  // namespace phr

@@ -288,6 +288,7 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
         P.redo_list[k] = pid;
         const uint64_t need_full = pair_need(m, n, nb, G, make_band(m, n, nb, 1, 0));
         atomicMax(P.redo_need_max, static_cast<unsigned long long>(need_full));
+        if (P.redo_need) P.redo_need[k] = need_full;
     }
 
     // ---- traceback: every group walks its own pair, all groups in lockstep ----------
@@ -441,15 +442,16 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
 }
 
 template <class S>
-__global__ void __launch_bounds__(256) myers_kernel(ExtendParams P) {
+__global__ void __launch_bounds__(256, 3) myers_kernel(ExtendParams P) {
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    uint8_t* slot = P.scratch + warp_global * P.slot_bytes;
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
         task = __shfl_sync(PHR_FULL_MASK, task, 0);
         if (task >= P.tasks.range[1]) break;
+        uint8_t* slot = P.task_off ? P.scratch + P.task_off[task] : P.scratch + warp_global * P.slot_bytes;
+        const uint64_t slot_bytes = P.task_off ? P.task_len[task] : P.slot_bytes;
         const int G = P.tasks.task_group[task];
         const int count = P.tasks.task_count[task];
         const int grp = lane / G;
@@ -470,7 +472,7 @@ __global__ void __launch_bounds__(256) myers_kernel(ExtendParams P) {
             if (g < grp) excl += v;
             total += v;
         }
-        const bool fits = total <= P.slot_bytes;
+        const bool fits = total <= slot_bytes;
         if (!__any_sync(PHR_FULL_MASK, mine)) continue;
         myers_group<S>(P, d, pid, mine, G, slot, excl, fits);
     }

@@ -70,6 +70,7 @@ __device__ __forceinline__ void report_redo(const ExtendParams& P, uint32_t pid,
     const uint32_t k = atomicAdd(P.redo_count, 1u);
     P.redo_list[k] = pid;
     atomicMax(P.redo_need_max, static_cast<unsigned long long>(need));
+    if (P.redo_need) P.redo_need[k] = need;
 }
 
 // ===========================================================================
@@ -94,12 +95,17 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
     const uint32_t* qb = seq_base<S>(P, d.q_word);
     const uint32_t* tb = seq_base<S>(P, d.t_word);
 
-    // region: [runs (qn+tn+2) u32][hv int32 cells][hr u32 cells]
+    // region: [runs (qn+tn+2) u32][two value frames of qn+tn+1 int32][hr u32 cells]
+    // Later scores only read the previous frame's values, so values live in two
+    // ping-pong frames; the traceback reads only hr = raw << 2 | op of every frame.
     uint32_t* runs = reinterpret_cast<uint32_t*>(region);
     const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
-    const uint64_t cell_cap = region_bytes > runs_bytes ? (region_bytes - runs_bytes) / 8 : 0;
-    int32_t* hv = reinterpret_cast<int32_t*>(region + runs_bytes);
-    uint32_t* hr = reinterpret_cast<uint32_t*>(hv + cell_cap);
+    const uint64_t frame_bytes = align16(static_cast<uint64_t>(qn + tn + 1) * 4);
+    const uint64_t fixed = runs_bytes + 2 * frame_bytes;
+    const uint64_t cell_cap = region_bytes > fixed ? (region_bytes - fixed) / 4 : 0;
+    int32_t* hv_frames = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* hr = reinterpret_cast<uint32_t*>(region + fixed);
+    auto hvf = [&](int sc) -> int32_t* { return hv_frames + (sc & 1) * (frame_bytes / 4); };
 
     // largest score whose frames fit: lin_base(s+1) <= cell_cap
     const int max_s = qn + tn;
@@ -116,12 +122,12 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
     }
     if (alive && gl == 0) {
         const int32_t v = wfa_extend<S>(qb, qn, tb, tn, 0, 0);
-        hv[0] = v;
+        hvf(0)[0] = v;
         hr[0] = 0;
     }
     __syncwarp();
     if (alive) {
-        const int32_t v0 = hv[0];
+        const int32_t v0 = hvf(0)[0];
         if (!fitting) {
             if (qn - tn == 0 && v0 == qn) {  // wfa_simd.rs:277-283 (perfect match only on diagonal 0)
                 done = true;
@@ -159,6 +165,8 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
         const bool go = run && alive;
         int best_end_k = INT32_MAX;
         if (go) {
+            const int32_t* pv_frame = hvf(s - 1);
+            int32_t* cur_frame = hvf(s);
             // lane gl handles diagonals k with (k + tn) % G == gl
             int k = lo + ((gl - ((lo + tn) % G)) % G + G) % G;
             for (; k <= hi; k += G) {
@@ -167,7 +175,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
                 bool have = false;
                 // candidates in order [mismatch, ins, del]; the LAST maximal one wins
                 if (k >= plo && k <= phi) {
-                    const int32_t pv = hv[pbase + (k - plo)];
+                    const int32_t pv = pv_frame[k - plo];
                     if (pv != UNSET) {
                         best_pos = pv + 1;
                         best_op = 1;
@@ -175,7 +183,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
                     }
                 }
                 if (k > -tn && k - 1 >= plo && k - 1 <= phi) {
-                    const int32_t pv = hv[pbase + (k - 1 - plo)];
+                    const int32_t pv = pv_frame[k - 1 - plo];
                     if (pv != UNSET) {
                         const int32_t c = pv + 1;
                         if (!have || c >= best_pos) {
@@ -186,7 +194,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
                     }
                 }
                 if (k < qn && k + 1 >= plo && k + 1 <= phi) {
-                    const int32_t pv = hv[pbase + (k + 1 - plo)];
+                    const int32_t pv = pv_frame[k + 1 - plo];
                     if (pv != UNSET) {
                         if (!have || pv >= best_pos) {
                             best_pos = pv;
@@ -204,7 +212,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
                         aux = (static_cast<uint32_t>(best_pos) << 2) | best_op;
                     }
                 }
-                hv[base + (k - lo)] = val;
+                cur_frame[k - lo] = val;
                 hr[base + (k - lo)] = aux;
                 if (val != UNSET) {
                     if (!fitting) {
@@ -230,7 +238,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
     if (act && overflow && gl == 0) {
         // retry with room for twice the scores reached so far (capped at the full search)
         const int64_t s2 = ::min(static_cast<long long>(max_s) + 1, 2LL * s + 64);
-        const uint64_t need = align16(static_cast<uint64_t>(qn + tn + 2) * 4) + lin_base(s2, qn, tn) * 8 + 64;
+        const uint64_t need = fixed + lin_base(s2, qn, tn) * 4 + 64;
         report_redo(P, pid, need);
     }
 
@@ -303,6 +311,280 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
         } else if (trace && ovf) {
             atomicOr(P.error_flag, 2u);
         }
+    }
+}
+
+// ===========================================================================
+// Linear WFA, one CTA per pair (long pairs)
+// ===========================================================================
+// A warp-per-pair wavefront on a long, divergent pair is latency-bound: every cell is a
+// chain of dependent loads (previous frame, both sequences) and one warp cannot hide
+// them. Here a CTA of kBigThreads threads takes one pair; both sequences and, while they
+// fit, the two value frames live in shared memory; the history (hr) goes to the pair's
+// scratch region with coalesced stores (consecutive diagonals on consecutive threads).
+// Frames that outgrow shared memory move to the region's global frames, the same layout
+// the warp kernel uses, so scratch needs and the redo rule are identical.
+
+// 32 bits holding symbols [pos, pos + kPerWord) of a sequence staged in shared memory.
+template <class S>
+__device__ __forceinline__ uint32_t window_sm(const uint32_t* base, int32_t pos) {
+    const uint32_t w = static_cast<uint32_t>(pos) / S::kPerWord;
+    const uint32_t sh = (static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits;
+    return __funnelshift_r(base[w], base[w + 1], sh);
+}
+
+template <class S>
+__device__ __forceinline__ int32_t extend_sm(const uint32_t* q, int32_t qn, const uint32_t* t, int32_t tn,
+                                             int32_t q_pos, int32_t k) {
+    const int32_t j = q_pos - k;
+    if (q_pos < 0 || q_pos >= qn || j < 0 || j >= tn) return q_pos;
+    const int32_t lim = min(qn - q_pos, tn - j);
+    int32_t n = 0;
+    while (n < lim) {
+        const uint32_t x = window_sm<S>(q, q_pos + n) ^ window_sm<S>(t, j + n);
+        if (x != 0) {
+            n += (__ffs(x) - 1) / S::kBits;
+            return q_pos + (n < lim ? n : lim);
+        }
+        n += S::kPerWord;
+    }
+    return q_pos + lim;
+}
+
+template <class S>
+__device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
+                               uint64_t region_bytes, uint32_t* sm, uint32_t sm_words, int* sh_end) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int qn = d.qn, tn = d.tn;
+    const bool fitting = tn > qn + qn / 2 + 10;
+
+    // ---- stage both sequences (plus one zero word each) in shared memory ----
+    const uint32_t* gq = seq_base<S>(P, d.q_word);
+    const uint32_t* gt = seq_base<S>(P, d.t_word);
+    const int qw = (qn + S::kPerWord - 1) / S::kPerWord;
+    const int tw = (tn + S::kPerWord - 1) / S::kPerWord;
+    uint32_t* sq = sm;
+    uint32_t* st = sm + qw + 1;
+    for (int i = tid; i <= qw; i += nthr) sq[i] = i < qw ? __ldg(gq + i) : 0u;
+    for (int i = tid; i <= tw; i += nthr) st[i] = i < tw ? __ldg(gt + i) : 0u;
+    const uint32_t fr_off = (static_cast<uint32_t>(qw + tw + 2) + 3) & ~3u;
+    const uint32_t fcap = sm_words > fr_off ? (sm_words - fr_off) / 2 : 0;  // cells per shared frame
+    int32_t* sfr = reinterpret_cast<int32_t*>(sm + fr_off);
+
+    // ---- region layout, as in wfa_linear_group ----
+    uint32_t* runs = reinterpret_cast<uint32_t*>(region);
+    const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
+    const uint64_t frame_bytes = align16(static_cast<uint64_t>(qn + tn + 1) * 4);
+    const uint64_t fixed = runs_bytes + 2 * frame_bytes;
+    const uint64_t cell_cap = region_bytes > fixed ? (region_bytes - fixed) / 4 : 0;
+    int32_t* gfr = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* hr = reinterpret_cast<uint32_t*>(region + fixed);
+    bool global_frames = false;
+    auto frame = [&](int sc) -> int32_t* {
+        return global_frames ? gfr + (sc & 1) * (frame_bytes / 4) : sfr + (sc & 1) * fcap;
+    };
+
+    if (tid < 3) sh_end[tid] = INT32_MAX;
+    const int max_s = qn + tn;
+    bool done = false, overflow = false;
+    int s_end = 0, t_end = 0, s = 1;
+    if (lin_base(1, qn, tn) > cell_cap) overflow = true;
+    if (fcap < 1) global_frames = true;
+    __syncthreads();
+    if (!overflow) {
+        if (tid == 0) {
+            frame(0)[0] = extend_sm<S>(sq, qn, st, tn, 0, 0);
+            hr[0] = 0;
+        }
+        __syncthreads();
+        const int32_t v0 = frame(0)[0];
+        if (!fitting) {
+            if (qn - tn == 0 && v0 == qn) {  // wfa_simd.rs:277-283
+                done = true;
+                t_end = tn;
+            }
+        } else if (qn <= tn && v0 >= qn) {
+            done = true;
+            t_end = qn;
+        }
+        for (; !done && s <= max_s; ++s) {
+            const int lo = -min(s, tn), hi = min(s, qn);
+            const int plo = -min(s - 1, tn), phi = min(s - 1, qn);
+            const uint64_t base = lin_base(s, qn, tn);
+            const int width = hi - lo + 1;
+            if (base + static_cast<uint64_t>(width) > cell_cap) {
+                overflow = true;
+                break;
+            }
+            if (!global_frames && static_cast<uint32_t>(width) > fcap) {
+                // frames outgrow shared memory: continue on the region's global frames
+                const int32_t* src = frame(s - 1);
+                int32_t* dst = gfr + ((s - 1) & 1) * (frame_bytes / 4);
+                for (int i = tid; i < phi - plo + 1; i += nthr) dst[i] = src[i];
+                global_frames = true;
+                __syncthreads();
+            }
+            const int32_t* pv_frame = frame(s - 1);
+            int32_t* cur_frame = frame(s);
+            if (tid == 0) sh_end[(s + 1) % 3] = INT32_MAX;
+            int my_end = INT32_MAX;
+            for (int k = lo + tid; k <= hi; k += nthr) {
+                int32_t best_pos = UNSET;
+                uint32_t best_op = 0;
+                bool have = false;
+                // candidates in order [mismatch, ins, del]; the LAST maximal one wins
+                if (k >= plo && k <= phi) {
+                    const int32_t pv = pv_frame[k - plo];
+                    if (pv != UNSET) {
+                        best_pos = pv + 1;
+                        best_op = 1;
+                        have = true;
+                    }
+                }
+                if (k > -tn && k - 1 >= plo && k - 1 <= phi) {
+                    const int32_t pv = pv_frame[k - 1 - plo];
+                    if (pv != UNSET) {
+                        const int32_t c = pv + 1;
+                        if (!have || c >= best_pos) {
+                            best_pos = c;
+                            best_op = 2;
+                            have = true;
+                        }
+                    }
+                }
+                if (k < qn && k + 1 >= plo && k + 1 <= phi) {
+                    const int32_t pv = pv_frame[k + 1 - plo];
+                    if (pv != UNSET) {
+                        if (!have || pv >= best_pos) {
+                            best_pos = pv;
+                            best_op = 3;
+                            have = true;
+                        }
+                    }
+                }
+                int32_t val = UNSET;
+                uint32_t aux = 0;
+                if (have) {
+                    const int32_t j = best_pos - k;
+                    if (!(best_pos < 0 || best_pos > qn || j < 0 || j > tn)) {
+                        val = extend_sm<S>(sq, qn, st, tn, best_pos, k);
+                        aux = (static_cast<uint32_t>(best_pos) << 2) | best_op;
+                    }
+                }
+                cur_frame[k - lo] = val;
+                hr[base + (k - lo)] = aux;
+                if (val != UNSET) {
+                    if (!fitting) {
+                        if (k == qn - tn && val >= qn) my_end = k;
+                    } else if (k >= qn - tn && k <= qn && val >= qn) {
+                        my_end = min(my_end, k);
+                    }
+                }
+            }
+            my_end = __reduce_min_sync(PHR_FULL_MASK, my_end);
+            if ((tid & 31) == 0 && my_end != INT32_MAX) atomicMin(&sh_end[s % 3], my_end);
+            __syncthreads();
+            const int kk = sh_end[s % 3];
+            if (kk != INT32_MAX) {
+                done = true;
+                s_end = s;
+                t_end = qn - kk;
+            }
+        }
+    }
+    if (done && s_end == 0) s = 0;
+    const bool failed = !done && !overflow;
+    if (overflow && tid == 0) {
+        const int64_t s2 = ::min(static_cast<long long>(max_s) + 1, 2LL * s + 64);
+        report_redo(P, pid, fixed + lin_base(s2, qn, tn) * 4 + 64);
+    }
+
+    // ---- traceback (wfa_simd.rs:959-1041) by thread 0, formatting by warp 0 ----
+    if (tid < 32) {
+        RunWriter rw;
+        rw.init(runs, static_cast<uint32_t>(qn + tn + 2));
+        if (done && tid == 0) {
+            int qi = qn, ti = t_end, k = qi - ti, ss = s_end;
+            while (qi > 0 || ti > 0) {
+                if (ss < 0) break;
+                if (ss == 0) {
+                    const int mm = min(qi, ti);
+                    rw.push(0, static_cast<uint32_t>(mm));
+                    qi -= mm;
+                    ti -= mm;
+                    break;
+                }
+                const int lo = -min(ss, tn);
+                const uint32_t aux = hr[lin_base(ss, qn, tn) + (k - lo)];
+                const uint32_t op = aux & 3;
+                const int32_t edit_start = static_cast<int32_t>(aux >> 2);
+                const int mc = qi - edit_start;
+                if (mc > 0) {
+                    rw.push(0, static_cast<uint32_t>(mc));
+                    qi -= mc;
+                    ti -= mc;
+                }
+                if (op == 1) {
+                    rw.push(1, 1);
+                    --qi;
+                    --ti;
+                } else if (op == 2) {
+                    rw.push(3, 1);
+                    --qi;
+                    k -= 1;
+                } else if (op == 3) {
+                    rw.push(2, 1);
+                    --ti;
+                    k += 1;
+                }
+                --ss;
+            }
+            rw.flush();
+        }
+        const uint32_t nr = __shfl_sync(PHR_FULL_MASK, rw.n, 0);
+        const bool ovf = __shfl_sync(PHR_FULL_MASK, rw.overflow ? 1 : 0, 0) != 0;
+        __syncwarp();
+        const uint32_t tl = format_group(runs, (done && !ovf) ? nr : 0, P.text + P.text_off[pid], 32);
+        if (tid == 0) {
+            if (done && !ovf) {
+                PairOut o;
+                o.status = PHR_OK;
+                o.ed = s_end;
+                o.t_consumed = t_end;
+                o.affine_score = 0;
+                o.n_runs = nr;
+                o.text_len = tl;
+                P.out[pid] = o;
+            } else if (failed) {
+                PairOut o = {};
+                o.status = PHR_ALIGNMENT_FAILED;
+                P.out[pid] = o;
+            } else if (done && ovf) {
+                atomicOr(P.error_flag, 2u);
+            }
+        }
+    }
+    __syncthreads();  // shared memory and the task slot are reused by the next pair
+}
+
+template <class S>
+__global__ void __launch_bounds__(kBigThreads, 2) wfa_linear_big_kernel(ExtendParams P) {
+    extern __shared__ __align__(16) uint32_t big_sm[];
+    __shared__ uint32_t sh_task;
+    __shared__ int sh_end[3];
+    const uint32_t sm_words = P.big_smem / 4;
+    for (;;) {
+        if (threadIdx.x == 0) sh_task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
+        __syncthreads();
+        const uint32_t task = sh_task;
+        __syncthreads();
+        if (task >= P.tasks.range[1]) break;
+        if (!(P.tasks.task_group[task] & kBigTask)) continue;
+        const uint32_t pid = P.tasks.order[P.tasks.task_first[task]];
+        const PairDesc d = P.desc[pid];
+        if (d.mode != (S::kBits == 2 ? 0 : 1)) continue;
+        wfa_linear_cta<S>(P, d, pid, P.scratch + P.task_off[task], P.task_len[task] & ~15ull, big_sm, sm_words,
+                          sh_end);
     }
 }
 
@@ -663,13 +945,16 @@ template <class S, bool kAffine>
 __global__ void __launch_bounds__(256) wfa_kernel(ExtendParams P) {
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    uint8_t* slot = P.scratch + warp_global * P.slot_bytes;
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
         task = __shfl_sync(PHR_FULL_MASK, task, 0);
         if (task >= P.tasks.range[1]) break;
-        const int G = P.tasks.task_group[task];
+        uint8_t* slot = P.task_off ? P.scratch + P.task_off[task] : P.scratch + warp_global * P.slot_bytes;
+        const uint64_t slot_bytes = P.task_off ? P.task_len[task] : P.slot_bytes;
+        const uint8_t tg = P.tasks.task_group[task];
+        if (tg & kBigTask) continue;  // a redo task of wfa_linear_big_kernel
+        const int G = tg;
         const int count = P.tasks.task_count[task];
         const int grp = lane / G;
         bool act = grp < count;
@@ -678,9 +963,21 @@ __global__ void __launch_bounds__(256) wfa_kernel(ExtendParams P) {
         if (act) d = P.desc[pid];
         // pairs of the other symbol mode run in the other instantiation
         act = act && d.mode == (S::kBits == 2 ? 0 : 1);
+        // long linear pairs run one per CTA: deferred from the main pass to the redo
+        // passes, where wfa_linear_big_kernel takes them
+        if (!kAffine && act && !P.task_off && big_pair(P.engine, P.big_min, P.big_smem, d.qn, d.tn, d.mode)) {
+            if ((lane & (G - 1)) == 0) report_redo(P, pid, wfa_region_est(d.qn, d.tn, false));
+            act = false;
+        }
         if (!__any_sync(PHR_FULL_MASK, act)) continue;
-        const uint64_t region_bytes = (P.slot_bytes / (32 / G)) & ~15ull;
+        // redo tasks hold one pair, which gets the whole task region
+        const uint64_t region_bytes = (P.task_off ? slot_bytes : slot_bytes / (32 / G)) & ~15ull;
         uint8_t* region = slot + static_cast<uint64_t>(grp) * region_bytes;
+        // a task whose estimated need exceeds the slot goes straight to a redo pass
+        if (!P.task_off && P.task_need && P.task_need[task] > slot_bytes) {
+            if (act && (lane & (G - 1)) == 0) report_redo(P, pid, P.task_need[task] / (32 / G));
+            continue;
+        }
         if (kAffine)
             wfa_affine_group<S>(P, d, pid, act, G, region, region_bytes);
         else
@@ -695,6 +992,17 @@ void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t 
 }
 void launch_wfa_linear_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st) {
     wfa_kernel<SeqB, false><<<grid, block, 0, st>>>(p);
+}
+void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream_t st) {
+    if (mode == 0) {
+        cudaFuncSetAttribute(wfa_linear_big_kernel<Seq2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(p.big_smem));
+        wfa_linear_big_kernel<Seq2><<<grid, kBigThreads, p.big_smem, st>>>(p);
+    } else {
+        cudaFuncSetAttribute(wfa_linear_big_kernel<SeqB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(p.big_smem));
+        wfa_linear_big_kernel<SeqB><<<grid, kBigThreads, p.big_smem, st>>>(p);
+    }
 }
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st) {
     wfa_kernel<Seq2, true><<<grid, block, 0, st>>>(p);

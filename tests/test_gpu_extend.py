@@ -150,3 +150,53 @@ def test_percall_matches_batched(eng):
         a1, c1 = eng.extend_packed(e, packed)
         a2, c2 = eng.extend_packed(e, packed, percall=True)
         assert P.unpack(a1, c1) == P.unpack(a2, c2)
+
+
+def long_linear_pairs():
+    """Pairs long enough for the CTA-per-pair linear WFA kernel (qlen+tlen >= 4096)."""
+    rng = np.random.default_rng(21)
+    packed = D.extension_pairs(40, 2100, 12000, 0.08, seed=21)
+    pairs = [(bytes(packed.seq[packed.q_off[i]:packed.q_off[i] + packed.q_len[i]]),
+              bytes(packed.seq[packed.t_off[i]:packed.t_off[i] + packed.t_len[i]])) for i in range(packed.n)]
+    for i in range(12):  # fitting branch: read inside a window more than 1.5x its length
+        t = bytes(rng.choice(list(b"ACGT"), 7000).tolist())
+        s = int(rng.integers(0, 3000))
+        q = bytearray(t[s:s + 2600])
+        for _ in range(int(rng.integers(0, 120))):
+            q[int(rng.integers(0, len(q)))] = int(rng.choice(list(b"ACGT")))
+        pairs.append((bytes(q), t, 0, s if i % 2 else 0))
+    for L in (2500, 5000):  # unrelated: scores near half the length, widest frames
+        pairs.append((bytes(rng.choice(list(b"ACGT"), L).tolist()), bytes(rng.choice(list(b"ACGT"), L + 100).tolist())))
+    q = bytes(rng.choice(list(b"ACGT"), 6000).tolist())
+    pairs.append((q, q))                                     # identical
+    qb = bytearray(q)
+    for p in rng.integers(0, 6000, 40):
+        qb[int(p)] = ord("N")
+    pairs.append((bytes(qb), q.lower()))                     # byte path: N and lowercase
+    pairs.append((bytes(qb[:3000]), bytes(qb)))              # byte path, fitting
+    return pairs
+
+
+def test_long_linear_pairs_cta_kernel(eng):
+    pairs = long_linear_pairs()
+    assert eng.get_tune("wfa_big_min") > 0
+    compare(eng, A.ENGINE_WFA_LINEAR, pairs)
+    # small shared memory: frames of the widest pairs move to global memory mid-run
+    with P.Engine(0) as e2:
+        e2.set_tune("wfa_big_smem", 40 << 10)
+        compare(e2, A.ENGINE_WFA_LINEAR, pairs)
+        # CTA kernel off: the warp-per-pair kernel on the same pairs
+        e2.set_tune("wfa_big_min", 0)
+        compare(e2, A.ENGINE_WFA_LINEAR, pairs)
+
+
+def test_tune_keys_validated(eng):
+    with pytest.raises(P.EngineError):
+        eng.set_tune("no_such_key", 1)
+    with pytest.raises(P.EngineError):
+        eng.set_tune("wfa_group_long", 3)
+    with pytest.raises(P.EngineError):
+        eng.set_tune("block_threads", 512)
+    before = eng.get_tune("myers_band_base")
+    eng.set_tune("myers_band_base", before)
+    assert eng.get_tune("myers_band_base") == before
