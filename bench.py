@@ -243,7 +243,8 @@ def run_engine(args, rank, world):
     # per-kernel device times (CUDA events on the launching stream)
     recs = (A.KernelTiming * 64)()
     nrec = L.phr_ctx_get_timing(eng.handle, recs, 64)
-    ktimes = {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(min(nrec, 64))}
+    ktimes = {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(min(nrec, 64))
+              if not recs[i].name.startswith(b"host:")}
 
     # ---- end to end through the host API, pinned host buffers ----------------
     def pinned_pairs(p):
@@ -302,6 +303,8 @@ def run_engine(args, rank, world):
     # kernel families: main pass, byte-mode instantiation and redo passes of one engine
     fam = {}
     for k, (nlk, totk) in ktimes.items():
+        if k.startswith("host:"):
+            continue
         f = next((p for p in ("myers", "wfa_affine", "wfa_linear") if k.startswith(p)), k)
         a = fam.setdefault(f, [0, 0.0])
         a[0] += nlk
@@ -392,37 +395,44 @@ def run_pipeline(eng, dev, args):
     order = rng.permutation(len(stream))
     stream = [stream[i] for i in order]
     is_short = [len(r) <= 500 for r in stream]
-    gaps = rng.exponential(1.0 / args.served_rate, len(stream))
-    srv = eng.server(idx, strategy=A.BALANCED, max_batch_reads=2048, max_wait_us=1000, n_streams=3)
-    # warm the workers
-    for r in stream[:64]:
-        srv.submit(r)
-    got = 0
-    while got < 64:
-        got += len(srv.poll(4096, wait_us=20000))
-    lat = {}
-    ids = {}
-    t_start = time.perf_counter()
-    next_t = t_start
-    i = 0
-    done = 0
-    while done < len(stream):
-        now = time.perf_counter()
-        while i < len(stream) and next_t <= now:
-            ids[srv.submit(stream[i])] = i
-            next_t += gaps[i]
-            i += 1
-        for rid, res, l in srv.poll(4096, wait_us=200 if i >= len(stream) else 0):
-            lat[ids[rid]] = l
-            done += 1
-    t_total = time.perf_counter() - t_start
-    srv.close()
-    sl = sorted(lat[j] for j in range(len(stream)) if is_short[j])
-    al = sorted(lat.values())
-    out["served"] = {"rate_offered_reads_per_s": args.served_rate, "reads": len(stream), "long_reads": n_long,
-                     "throughput_reads_per_s": len(stream) / t_total,
-                     "p50_ms_150bp": sl[len(sl) // 2] / 1000.0, "p99_ms_150bp": sl[int(len(sl) * 0.99)] / 1000.0,
-                     "p99_ms_all": al[int(len(al) * 0.99)] / 1000.0}
+
+    def serve(rate):
+        gaps = np.random.default_rng(104).exponential(1.0 / rate, len(stream))
+        arrive = np.cumsum(gaps)
+        srv = eng.server(idx, strategy=A.BALANCED, max_batch_reads=2048, max_wait_us=1000, n_streams=3)
+        srv.submit_many(stream[:64])  # warm the workers
+        got = 0
+        while got < 64:
+            got += len(srv.poll(4096, wait_us=20000))
+        lat = {}
+        ids = {}
+        t_start = time.perf_counter()
+        i = 0
+        done = 0
+        while done < len(stream):
+            now = time.perf_counter() - t_start
+            j = int(np.searchsorted(arrive, now, side="right"))
+            if j > i:  # every read whose arrival time has passed, in one call
+                for k, rid in enumerate(srv.submit_many(stream[i:j])):
+                    ids[rid] = i + k
+                i = j
+            for rid, res, l in srv.poll(4096, wait_us=200 if i >= len(stream) else 0):
+                lat[ids[rid]] = l
+                done += 1
+        t_total = time.perf_counter() - t_start
+        srv.close()
+        sl = sorted(lat[j] for j in range(len(stream)) if is_short[j])
+        al = sorted(lat.values())
+        return {"rate_offered_reads_per_s": rate, "reads": len(stream), "long_reads": n_long,
+                "throughput_reads_per_s": len(stream) / t_total,
+                "p50_ms_150bp": sl[len(sl) // 2] / 1000.0, "p99_ms_150bp": sl[int(len(sl) * 0.99)] / 1000.0,
+                "p99_ms_all": al[int(len(al) * 0.99)] / 1000.0}
+
+    sweep = [serve(r) for r in args.served_rates]
+    ok = [x for x in sweep if x["p99_ms_150bp"] <= 50.0]
+    best = max(ok, key=lambda x: x["throughput_reads_per_s"]) if ok else max(sweep, key=lambda x: x["rate_offered_reads_per_s"])
+    out["served"] = dict(best, p99_target_ms=50.0, meets_p99_target=bool(ok))
+    out["served_sweep"] = sweep
     out["served_over_percall"] = out["served"]["throughput_reads_per_s"] / out["percall_balanced_reads_per_s"]
     out["workload"] = ("align_read, 1 Mbp i.i.d. reference, 150 bp reads both strands, 1 % subs + 0.05 % "
                        "1-3 bp indels; served: Poisson arrivals, 90 % 150 bp + 10 % lognormal long reads")
@@ -440,7 +450,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-pipeline", action="store_true", help="skip the read-pipeline / serving section")
     ap.add_argument("--reads", type=int, default=20000, help="reads of the read-pipeline section")
-    ap.add_argument("--served-rate", type=float, default=100000.0, help="Poisson arrival rate (reads/s)")
+    ap.add_argument("--served-rates", type=float, nargs="+", default=[25000.0, 50000.0, 100000.0],
+                    help="Poisson arrival rates (reads/s) of the served sweep")
     ap.add_argument("--traffic-gb-per-step", type=float, default=None,
                     help="DRAM bytes per step of the dominant kernel from an ncu capture (reported as is)")
     args = ap.parse_args()

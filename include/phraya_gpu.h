@@ -130,6 +130,8 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *   "wfa_big_min"                        linear WFA pairs with qlen+tlen >= this run one
  *                                        per CTA (0 = never)
  *   "wfa_big_smem"                       shared memory of that kernel, bytes (16 KiB..200 KiB)
+ *   "max_blocks_per_sm"                  resident blocks per SM of the persistent extension
+ *                                        kernels (1..4)
  * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune
  * file (written by the autotuner); unknown keys and bad values there are ignored. */
 phr_status phr_ctx_set_tune(phr_ctx* ctx, const char* key, int64_t value);
@@ -417,6 +419,12 @@ typedef struct {
     uint64_t hbm_reserve_bytes;    /* free HBM kept back when admitting (0 = 2 GiB) */
     uint32_t max_wait_us;          /* batch-forming window after first arrival     */
     uint32_t n_streams;            /* concurrent batches in flight (0 = 2)         */
+    int32_t short_lane;            /* worker 0 takes only reads <= 500 bases, on a
+                                      high-priority stream: 0 = on when n_streams >= 2,
+                                      1 = on, -1 = off                               */
+    uint32_t long_blocks_per_sm;   /* resident blocks per SM of the extension kernels
+                                      of the other workers while a short lane runs
+                                      (0 = 2; the short lane keeps the rest)        */
 } phr_server_config;
 
 typedef struct {
@@ -435,6 +443,11 @@ phr_status phr_server_create(phr_ctx* ctx, const phr_index* idx, const phr_serve
 /* Enqueues one read (bytes copied); returns its request id in *request_id. */
 phr_status phr_server_submit(phr_server* srv, const uint8_t* read, uint32_t len,
                              uint64_t* request_id);
+/* Enqueues n reads (read i = seq[off[i] .. off[i] + len[i]), bytes copied) with one
+ * lock round trip; their request ids are written to ids[0..n). Each read's latency
+ * starts at this call. */
+phr_status phr_server_submit_many(phr_server* srv, const uint8_t* seq, const uint64_t* off,
+                                  const uint32_t* len, uint64_t n, uint64_t* ids);
 /*
  * Copies up to `max_results` finished requests into `res` (and their alignments and
  * CIGARs, packed, into the given arrays), returns how many in *n_out.

@@ -206,6 +206,8 @@ class ServerConfig(C.Structure):
         ("hbm_reserve_bytes", C.c_uint64),
         ("max_wait_us", C.c_uint32),
         ("n_streams", C.c_uint32),
+        ("short_lane", C.c_int32),
+        ("long_blocks_per_sm", C.c_uint32),
     ]
 
 
@@ -259,6 +261,8 @@ PROTOTYPES = {
     "phr_server_create": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(ServerConfig),
                                       C.POINTER(C.c_void_p)]),
     "phr_server_submit": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "phr_server_submit_many": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                           C.c_void_p]),
     "phr_server_poll": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p,
                                     C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32)]),
     "phr_server_destroy": (C.c_int32, [C.c_void_p]),

@@ -306,11 +306,10 @@ def _align_packed(engine, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AF
     rr = np.zeros(max(n, 1), dtype=READ_RESULT_DTYPE)
     K = 1 if strategy == A.FAST else 2 if strategy == A.BALANCED else 50
     acap = 2 * K * n + 16
-    aln = np.zeros(acap, dtype=ALN_DTYPE)
-    maxlen = int(packed.len.max()) if n else 1
-    ccap = int(acap) * (6 * maxlen + 16)
-    ccap = min(ccap, 1 << 31)
-    cig = np.zeros(ccap, dtype=np.uint8)
+    aln = np.empty(acap, dtype=ALN_DTYPE)  # the library writes every entry it reports
+    # CIGAR text bound: 6 * len + 16 bytes per alignment of a read of length len
+    ccap = 2 * K * (6 * int(packed.len.astype(np.uint64).sum()) + 16 * n) + 64
+    cig = np.empty(ccap, dtype=np.uint8)
     arena = A.ReadResultArena(rr.ctypes.data, aln.ctypes.data, acap, 0, cig.ctypes.data, ccap, 0)
     stats = A.AlignStats()
     cfg = A.AlignConfig(strategy, gap_model)
@@ -361,17 +360,19 @@ class Server:
     """Continuous-batching read server over a device-resident index."""
 
     def __init__(self, engine, index, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, max_batch_reads=4096,
-                 max_batch_bases=0, max_wait_us=200, n_streams=2, hbm_reserve_bytes=0):
+                 max_batch_bases=0, max_wait_us=200, n_streams=2, hbm_reserve_bytes=0, short_lane=0,
+                 long_blocks_per_sm=0):
         self._eng = engine
         self._lib = engine._lib
         self._index = index
         cfg = A.ServerConfig(A.AlignConfig(strategy, gap_model), max_batch_reads, max_batch_bases, hbm_reserve_bytes,
-                             max_wait_us, n_streams)
+                             max_wait_us, n_streams, short_lane, long_blocks_per_sm)
         h = C.c_void_p()
         engine.check(self._lib.phr_server_create(engine.handle, index.handle, C.byref(cfg), C.byref(h)))
         self._h = h
         K = 1 if strategy == A.FAST else 2 if strategy == A.BALANCED else 50
         self._K = K
+        self._bufs = None
 
     def submit(self, read):
         rid = C.c_uint64()
@@ -381,19 +382,47 @@ class Server:
             raise EngineError(st, "phr_server_submit failed")
         return rid.value
 
+    def submit_many(self, reads):
+        """Enqueues several reads in one call; returns their request ids."""
+        n = len(reads)
+        if n == 0:
+            return []
+        lens = np.fromiter((len(r) for r in reads), dtype=np.uint32, count=n)
+        offs = np.zeros(n, dtype=np.uint64)
+        if n > 1:
+            np.cumsum(lens[:-1], out=offs[1:])
+        seq = b"".join(bytes(r) for r in reads)
+        ids = np.zeros(n, dtype=np.uint64)
+        st = self._lib.phr_server_submit_many(self._h, seq, offs.ctypes.data, lens.ctypes.data, n, ids.ctypes.data)
+        if st != A.PHR_OK:
+            raise EngineError(st, "phr_server_submit_many failed")
+        return ids.tolist()
+
     def poll(self, max_results=4096, wait_us=0, max_read_len=100000):
-        res = (A.ServerResult * max_results)()
+        """Finished requests: [(request_id, (outcome, has_result, reverse, alignments), latency_us)].
+        The result buffers are kept across calls; `max_read_len` bounds the CIGAR text of
+        one alignment (6 * len + 16 bytes)."""
         acap = max_results * 2 * self._K + 16
-        aln = np.zeros(acap, dtype=ALN_DTYPE)
-        ccap = acap * (6 * 1024 + 16)
-        cig = np.zeros(ccap, dtype=np.uint8)
+        ccap = max_results * self._K * (6 * max_read_len + 16)
+        ccap = min(ccap, 1 << 30)
+        if self._bufs is None or self._bufs[0] < max_results or self._bufs[2].size < acap or self._bufs[3].size < ccap:
+            self._bufs = (max_results, (A.ServerResult * max_results)(), np.empty(acap, dtype=ALN_DTYPE),
+                          np.empty(ccap, dtype=np.uint8))
+        _, res, aln, cig = self._bufs
         n = C.c_uint32()
-        st = self._lib.phr_server_poll(self._h, res, max_results, aln.ctypes.data, acap, cig.ctypes.data, ccap,
+        st = self._lib.phr_server_poll(self._h, res, max_results, aln.ctypes.data, aln.size, cig.ctypes.data, cig.size,
                                        wait_us, C.byref(n))
         if st not in (A.PHR_OK,):
             raise EngineError(st, "phr_server_poll failed")
         out = []
-        cb = cig.tobytes()
+        k = 0
+        used = 0
+        for i in range(n.value):
+            k += res[i].n_aln
+        if k:
+            ends = aln["cigar_off"][:k] + aln["cigar_len"][:k]
+            used = int(ends.max())
+        cb = cig[:used].tobytes()
         k = 0
         for i in range(n.value):
             r = res[i]

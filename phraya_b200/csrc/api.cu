@@ -133,6 +133,7 @@ phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out) 
         delete c;
         return PHR_ERR_CUDA;
     }
+    ctx->bind_stream();
     if (cfg && cfg->workspace_bytes) ctx->scratch_budget = cfg->workspace_bytes;
     if (cfg && cfg->tune_file_enable) {
         ctx->tune_file_enable = true;
@@ -156,6 +157,7 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "block_threads")) return &t.block_threads;
     if (!std::strcmp(key, "wfa_big_min")) return &t.wfa_big_min;
     if (!std::strcmp(key, "wfa_big_smem")) return &t.wfa_big_smem;
+    if (!std::strcmp(key, "max_blocks_per_sm")) return &t.max_blocks_per_sm;
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
@@ -165,6 +167,7 @@ bool tune_valid(const char* key, int64_t v) {
     if (!std::strcmp(key, "block_threads")) return v >= 32 && v <= 256 && v % 32 == 0;
     if (!std::strcmp(key, "wfa_big_min")) return v >= 0 && v <= INT32_MAX;
     if (!std::strcmp(key, "wfa_big_smem")) return v >= (16 << 10) && v <= (200 << 10) && v % 16 == 0;
+    if (!std::strcmp(key, "max_blocks_per_sm")) return v >= 1 && v <= 4;
     return false;
 }
 }  // namespace

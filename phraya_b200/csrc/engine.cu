@@ -18,14 +18,25 @@ namespace phr {
 // ---------------------------------------------------------------------------
 cudaError_t DeviceArena::reserve(size_t need) {
     if (need <= cap) return cudaSuccess;
-    if (base) cudaFree(base);
+    auto alloc = [&](size_t bytes) -> cudaError_t {
+        void* p = nullptr;
+        cudaError_t e = stream ? cudaMallocAsync(&p, bytes, stream) : cudaMalloc(&p, bytes);
+        base = static_cast<char*>(p);
+        return e;
+    };
+    if (base) {
+        if (stream)
+            cudaFreeAsync(base, stream);
+        else
+            cudaFree(base);
+    }
     base = nullptr;
     cap = 0;
     size_t want = std::max(need + need / 4, static_cast<size_t>(64) << 20);
-    cudaError_t e = cudaMalloc(&base, want);
+    cudaError_t e = alloc(want);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        e = cudaMalloc(&base, need);
+        e = alloc(need);
         if (e != cudaSuccess) {
             base = nullptr;
             return e;
@@ -35,6 +46,16 @@ cudaError_t DeviceArena::reserve(size_t need) {
     cap = want;
     used = 0;
     return cudaSuccess;
+}
+
+void Ctx::bind_stream() {
+    for (DeviceArena* a : {&arena, &scratch, &io, &pipe, &seeds}) a->stream = stream;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
 }
 
 void* DeviceArena::take(size_t bytes, size_t align) {
@@ -314,6 +335,8 @@ struct TaskBuild {
     unsigned long long* need_max;
     uint64_t* task_need;          // per task
     unsigned int* need_hist;      // 64 buckets by bit length of the need
+    int32_t big_min;              // linear WFA pairs for the CTA-per-pair kernel (not in the
+    uint32_t big_smem;            // main pass, so not in its slot statistics)
 };
 
 __device__ __forceinline__ int key_group(uint32_t k) { return 1 << ((k >> 28) & 7); }
@@ -358,7 +381,7 @@ __global__ void task_fill_kernel(TaskBuild T) {
         const PairDesc d = T.desc[T.order[p + c]];
         if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
             need += myers_need_est(d.qn, d.tn, G, T.band_base);
-        else
+        else if (!big_pair(T.engine, T.big_min, T.big_smem, d.qn, d.tn, d.mode))
             region = max(region, wfa_region_est(d.qn, d.tn, T.engine == PHR_ENGINE_WFA_AFFINE));
         ++cnt;
     }
@@ -368,7 +391,7 @@ __global__ void task_fill_kernel(TaskBuild T) {
     T.task_count[t] = static_cast<uint8_t>(cnt);
     T.task_group[t] = static_cast<uint8_t>(G);
     T.task_need[t] = need;
-    atomicAdd(&T.need_hist[64 - __clzll(need | 1)], 1u);
+    if (need) atomicAdd(&T.need_hist[64 - __clzll(need)], 1u);
     atomicMax(T.need_max, static_cast<unsigned long long>(need));
     if ((k >> 31) & 1) atomicMin(T.split_min, t);
 }
@@ -587,7 +610,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
 
     PHR_CUDA_TRY(ctx, cudaMemsetAsync(need_hist, 0, 64 * 4, st));
     TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, desc,
-                  engine, ctx->tune.myers_band_base, need_max, task_need, need_hist};
+                  engine, ctx->tune.myers_band_base, need_max, task_need, need_hist,
+                  ctx->tune.wfa_big_min, static_cast<uint32_t>(ctx->tune.wfa_big_smem)};
     {
         KernelScope ks(ctx, "task_head");
         task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
@@ -622,8 +646,10 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     PHR_CUDA_TRY(ctx, cudaGetLastError());
     {
-        const uint64_t n_tasks = h_ranges[3];
-        const uint64_t full_grid_warps = static_cast<uint64_t>(ctx->sm_count) * 4 * (ctx->tune.block_threads / 32);
+        uint64_t n_tasks = 0;  // tasks of the main pass with a scratch need
+        for (int b = 0; b < 64; ++b) n_tasks += h_hist[b];
+        const uint64_t full_grid_warps =
+            static_cast<uint64_t>(ctx->sm_count) * ctx->tune.max_blocks_per_sm * (ctx->tune.block_threads / 32);
         if (h_need * full_grid_warps > ctx->scratch_budget && n_tasks > 0) {
             uint64_t acc = 0, slot = 4096;
             for (int b = 0; b < 64; ++b) {
@@ -666,7 +692,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                            bool per_task = false, uint64_t per_task_total = 0,
                            uint64_t n_tasks_hint = 0) -> phr_status {
         const uint64_t warps_per_block = block / 32;
-        uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * 4;
+        uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * ctx->tune.max_blocks_per_sm;
         if (!per_task) {
             slot = std::max<uint64_t>((slot + 255) & ~255ull, 4096);
             // grid: resident blocks per SM, shrunk to the scratch budget
@@ -715,7 +741,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         }
         if (per_task && engine == PHR_ENGINE_WFA_LINEAR && P.big_min > 0 && n_tasks_hint > 0) {
             // long pairs of this redo list, one CTA each
-            const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, static_cast<uint64_t>(ctx->sm_count) * 2));
+            const uint64_t big_per_sm = ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1;
+            const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, ctx->sm_count * big_per_sm));
             PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 24, 0, 8, st));
             for (int mode = 0; mode < 2; ++mode) {
                 P.tasks.range = mode ? range1 : range0;
@@ -740,6 +767,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     std::vector<uint32_t> h_list;
     std::vector<unsigned long long> h_rneed;
     std::unordered_set<uint32_t> clamped;
+    HostScope hs_redo(ctx, "host:redo");
     for (int round = 0; round < 12; ++round) {
         uint32_t h_redo = 0;
         PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_redo, cnt + 7, 4, cudaMemcpyDeviceToHost, st));

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <string>
@@ -16,10 +17,14 @@ namespace phr {
 
 // Bump allocator over one growable device buffer. Reset per call; grown (free +
 // cudaMalloc) only between calls, when a call's precomputed need exceeds capacity.
+// Grow-only device buffer carved by take(). With a stream set, growth is stream-ordered
+// (cudaFreeAsync / cudaMallocAsync on that stream): it never waits for other streams,
+// so contexts sharing a device do not stall one another when one of them grows.
 struct DeviceArena {
     char* base = nullptr;
     size_t cap = 0;
     size_t used = 0;
+    cudaStream_t stream = nullptr;
     cudaError_t reserve(size_t need);
     void reset() { used = 0; }
     void* take(size_t bytes, size_t align = 256);
@@ -34,6 +39,7 @@ struct EngineTune {
     int block_threads = 256;
     int wfa_big_min = 4096;          // linear WFA pairs with qn+tn >= this run one per CTA (0: off)
     int wfa_big_smem = 100 << 10;    // shared memory of that kernel, bytes (two CTAs per SM)
+    int max_blocks_per_sm = 4;       // resident blocks per SM of the persistent extension kernels
 };
 
 struct Ctx {
@@ -65,6 +71,9 @@ struct Ctx {
     void begin_kernel(const char* name, cudaEvent_t* a);
     void end_kernel(const char* name, cudaEvent_t a);
     void resolve_timings();   // after a stream sync
+    // Binds the arenas to `stream` (stream-ordered growth) and keeps freed blocks cached in
+    // the device's default memory pool for the next growth.
+    void bind_stream();
     ~Ctx();
 };
 
@@ -79,6 +88,24 @@ struct KernelScope {
     }
     ~KernelScope() {
         if (ctx->timing && a) ctx->end_kernel(name, a);
+    }
+};
+
+// Wall-clock time of a host-side phase (GPU waits included), recorded under its name
+// in the same table as the kernels when timing is enabled.
+struct HostScope {
+    Ctx* ctx;
+    const char* name;
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    HostScope(Ctx* c, const char* n) : ctx(c), name(n), on(c->timing) {
+        if (on) t0 = std::chrono::steady_clock::now();
+    }
+    ~HostScope() {
+        if (!on) return;
+        auto& t = ctx->timings[name];
+        t.first += 1;
+        t.second += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
 };
 

@@ -1356,7 +1356,10 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
         r.cigar = out->eng_cigar[e];
         r.cigar_capacity = cap;
         phr_affine_costs costs{2, 4, 1};  // AffineCosts::default (wfa_simd.rs:537-539)
-        s = run_extend(ctx, slot_engine[e], dp, costs, &r, sum_qt_e[e]);
+        {
+            HostScope hs(ctx, "host:extend");
+            s = run_extend(ctx, slot_engine[e], dp, costs, &r, sum_qt_e[e]);
+        }
         if (s != PHR_OK) return s;
     }
     // ---- score_alignments + orientation choice ----
@@ -1467,6 +1470,7 @@ phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch
     if (has_st)
         for (uint64_t i = 0; i < n; ++i)
             if (rb->has_stored[i]) stored_total = std::max<uint64_t>(stored_total, rb->s_off[i] + rb->s_n[i]);
+    HostScope hs_all(ctx, "host:align_reads");
     DeviceArena& A = ctx->pipe;
     A.reset();
     PHR_CUDA_TRY(ctx, A.reserve(align_arena_need(n, rb->seq_bytes, stored_total) + rb->seq_bytes + n * 32));
@@ -1496,10 +1500,16 @@ phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch
         }
     }
     AlignOutput o;
-    phr_status s = align_reads_device(ctx, idx, d_seq, d_off, d_len, n, rb->seq_bytes, d_hs, d_so, d_sn, d_sv, d_sp,
-                                      cfg, &o);
+    phr_status s;
+    {
+        HostScope hs(ctx, "host:device_pipeline");
+        s = align_reads_device(ctx, idx, d_seq, d_off, d_len, n, rb->seq_bytes, d_hs, d_so, d_sn, d_sv, d_sp, cfg, &o);
+    }
     if (s != PHR_OK) return s;
-    s = pack_to_host(ctx, A, n, o, out, stats);
+    {
+        HostScope hs(ctx, "host:pack_to_host");
+        s = pack_to_host(ctx, A, n, o, out, stats);
+    }
     if (ctx->timing) ctx->resolve_timings();
     return s;
 }

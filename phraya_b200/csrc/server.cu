@@ -2,17 +2,23 @@
 //
 // No counterpart in the reference (phraya's CLI aligns files in batches of 4096 reads,
 // phraya-cli/src/main.rs:583-590). Requests are single reads. A scheduler thread forms
-// batches continuously: it takes the oldest pending request's length bucket (short
-// reads <= 500 bases ride the Myers path, long ones the WFA path), fills a batch from
-// that bucket up to max_batch_reads / max_batch_bases, and hands it to the first idle
-// worker once the device has the free memory the batch needs (cudaMemGetInfo minus the
-// configured reserve). Each worker owns a context (its own CUDA stream and device
-// arenas) and runs the whole align_read pipeline for its batch; workers overlap on the
-// device. The index is shared read-only. Results are queued with their latency
+// batches continuously from two length buckets (short reads <= 500 bases ride the Myers
+// path, long ones the WFA path): it fills a batch from one bucket up to
+// max_batch_reads / max_batch_bases and hands it to an idle worker once the device has
+// the free memory the batch needs (cudaMemGetInfo minus the configured reserve).
+//
+// Each worker owns a context (its own CUDA stream, device arenas and pinned host
+// buffers) and runs the whole align_read pipeline for its batch; workers overlap on the
+// device and the index is shared read-only. With a short lane, worker 0 takes only
+// short-read batches on a high-priority stream, and the other workers' persistent
+// extension kernels keep to long_blocks_per_sm resident blocks per SM, so a long batch
+// never holds every SM while short reads wait. Results are queued with their latency
 // (submit -> result ready) and handed out by phr_server_poll.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -44,6 +50,30 @@ struct Done {
 
 constexpr uint32_t kShortMax = 500;  // MYERS_MAX_QUERY_LEN (executor.rs:248)
 
+// Grow-only pinned host buffer (page-locked, so the worker's copies are truly async).
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t need) {
+        if (need <= cap) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max(need + need / 2, static_cast<size_t>(1) << 20);
+        if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        cap = want;
+        return true;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
 }  // namespace
 
 struct phr_server {
@@ -59,6 +89,7 @@ struct phr_server {
     uint64_t in_flight = 0;            // submitted, not yet completed
     uint64_t completions = 0;          // batches finished (admission waits on it)
     bool stopping = false;
+    bool short_lane = false;
     phr_status fatal = PHR_OK;
     std::string fatal_msg;
     struct Worker {
@@ -67,18 +98,61 @@ struct phr_server {
         std::vector<Request> batch;
         bool busy = false;
         bool has_work = false;
+        bool short_only = false;
+        int index = 0;
         std::condition_variable cv;
+        PinnedBuf seq, off, len, rr, aln, cig;
     };
     std::vector<Worker*> workers;
     std::thread scheduler;
+    // PHRAYA_SERVER_TRACE=<file>: one line per batch:
+    // worker bucket reads bases start_ms(since create) run_ms queued_ms(oldest read)
+    FILE* trace = nullptr;
+    std::mutex trace_mu;
+    Clock::time_point t_create;
 };
 
 namespace {
 
-uint64_t batch_bytes(const std::vector<Request>& b) {
-    uint64_t s = 0;
-    for (auto& r : b) s += r.seq.size();
-    return s;
+void finish_batch(phr_server* S, phr_server::Worker* W, std::vector<Request>& batch, phr_status st,
+                  const phr_read_result* rr, const phr_alignment* aln, const char* cig) {
+    const auto t1 = Clock::now();
+    const uint64_t n = batch.size();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (st != PHR_OK && S->fatal == PHR_OK) {
+            S->fatal = st;
+            S->fatal_msg = W->ctx.last_error;
+        }
+        for (uint64_t i = 0; i < n; ++i) {
+            Done d{};
+            d.res.request_id = batch[i].id;
+            d.res.latency_us = std::chrono::duration<double, std::micro>(t1 - batch[i].t0).count();
+            if (st == PHR_OK) {
+                d.res.outcome = rr[i].outcome;
+                d.res.has_result = rr[i].has_result;
+                d.res.reverse = rr[i].reverse;
+                d.res.n_aln = rr[i].n_aln;
+                for (uint32_t k = 0; k < rr[i].n_aln; ++k) {
+                    phr_alignment a = aln[rr[i].aln_off + k];
+                    const uint64_t co = d.cigar.size();
+                    d.cigar.append(cig + a.cigar_off, a.cigar_len);
+                    a.cigar_off = co;
+                    d.aln.push_back(a);
+                }
+            } else {
+                d.res.outcome = PHR_OUT_NO_ALIGNMENT;
+                d.res.has_result = 0;
+                d.res.n_aln = 0;
+            }
+            S->done.push_back(std::move(d));
+        }
+        S->in_flight -= n;
+        S->completions += 1;
+        W->busy = false;
+    }
+    S->cv_done.notify_all();
+    S->cv_work.notify_all();
 }
 
 void run_worker(phr_server* S, phr_server::Worker* W) {
@@ -92,66 +166,63 @@ void run_worker(phr_server* S, phr_server::Worker* W) {
             batch.swap(W->batch);
             W->has_work = false;
         }
-        // pack the batch and run align_read for all of it
+        // pack the batch into the worker's pinned buffers and run align_read on it
         const uint64_t n = batch.size();
-        std::vector<uint8_t> seq;
-        std::vector<uint64_t> off(n);
-        std::vector<uint32_t> len(n);
+        uint64_t bases = 0, maxlen = 1, cig_cap = 0;
+        const uint32_t K = S->cfg.align.strategy == PHR_FAST ? 1 : S->cfg.align.strategy == PHR_BALANCED ? 2 : 50;
+        for (auto& r : batch) {
+            bases += r.seq.size();
+            maxlen = std::max<uint64_t>(maxlen, r.seq.size());
+        }
+        const uint64_t acap = n * K + 16;
+        // CIGAR text: each alignment of a read of length L spans at most L query bases
+        // and, per the extension window, a bounded target stretch: 6 * L + 16 per alignment
+        for (auto& r : batch) cig_cap += K * (6 * r.seq.size() + 16);
+        cig_cap += 64;
+        if (!W->seq.ensure(bases + 64) || !W->off.ensure(n * 8) || !W->len.ensure(n * 4) ||
+            !W->rr.ensure(n * sizeof(phr_read_result)) || !W->aln.ensure(acap * sizeof(phr_alignment)) ||
+            !W->cig.ensure(cig_cap)) {
+            W->ctx.last_error = "pinned host buffer allocation failed";
+            finish_batch(S, W, batch, PHR_ERR_OOM, nullptr, nullptr, nullptr);
+            continue;
+        }
+        uint8_t* seq = W->seq.as<uint8_t>();
+        uint64_t* off = W->off.as<uint64_t>();
+        uint32_t* len = W->len.as<uint32_t>();
+        uint64_t o = 0;
         for (uint64_t i = 0; i < n; ++i) {
-            off[i] = seq.size();
+            off[i] = o;
             len[i] = static_cast<uint32_t>(batch[i].seq.size());
-            seq.insert(seq.end(), batch[i].seq.begin(), batch[i].seq.end());
+            if (len[i]) std::memcpy(seq + o, batch[i].seq.data(), len[i]);
+            o += len[i];
         }
         phr_read_batch rb{};
         rb.n_reads = n;
-        rb.seq = seq.data();
-        rb.seq_bytes = seq.size();
-        rb.off = off.data();
-        rb.len = len.data();
-        const uint32_t K = S->cfg.align.strategy == PHR_FAST ? 1 : S->cfg.align.strategy == PHR_BALANCED ? 2 : 50;
-        std::vector<phr_read_result> rr(n);
-        std::vector<phr_alignment> aln(n * K + 16);
-        uint64_t maxlen = 1;
-        for (auto l : len) maxlen = std::max<uint64_t>(maxlen, l);
-        std::vector<char> cig(aln.size() * (6 * maxlen + 16));
-        phr_read_result_arena ar{rr.data(), aln.data(), aln.size(), 0, cig.data(), cig.size(), 0};
-        phr_status st = phr::align_reads_host(&W->ctx, S->idx, &rb, S->cfg.align, &ar, nullptr);
-        const auto t1 = Clock::now();
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            if (st != PHR_OK && S->fatal == PHR_OK) {
-                S->fatal = st;
-                S->fatal_msg = W->ctx.last_error;
-            }
-            for (uint64_t i = 0; i < n; ++i) {
-                Done d{};
-                d.res.request_id = batch[i].id;
-                d.res.latency_us = std::chrono::duration<double, std::micro>(t1 - batch[i].t0).count();
-                if (st == PHR_OK) {
-                    d.res.outcome = rr[i].outcome;
-                    d.res.has_result = rr[i].has_result;
-                    d.res.reverse = rr[i].reverse;
-                    d.res.n_aln = rr[i].n_aln;
-                    for (uint32_t k = 0; k < rr[i].n_aln; ++k) {
-                        phr_alignment a = aln[rr[i].aln_off + k];
-                        const uint64_t co = d.cigar.size();
-                        d.cigar.append(cig.data() + a.cigar_off, a.cigar_len);
-                        a.cigar_off = co;
-                        d.aln.push_back(a);
-                    }
-                } else {
-                    d.res.outcome = PHR_OUT_NO_ALIGNMENT;
-                    d.res.has_result = 0;
-                    d.res.n_aln = 0;
-                }
-                S->done.push_back(std::move(d));
-            }
-            S->in_flight -= n;
-            S->completions += 1;
-            W->busy = false;
+        rb.seq = seq;
+        rb.seq_bytes = bases;
+        rb.off = off;
+        rb.len = len;
+        phr_read_result_arena ar{W->rr.as<phr_read_result>(), W->aln.as<phr_alignment>(), acap, 0,
+                                 W->cig.as<char>(), cig_cap, 0};
+        const auto tb0 = Clock::now();
+        const phr_status st = phr::align_reads_host(&W->ctx, S->idx, &rb, S->cfg.align, &ar, nullptr);
+        if (S->trace) {
+            const auto tb1 = Clock::now();
+            Clock::time_point oldest = batch.empty() ? tb0 : batch[0].t0;
+            for (auto& r : batch) oldest = std::min(oldest, r.t0);
+            std::lock_guard<std::mutex> lk(S->trace_mu);
+            std::string ph;
+            for (auto& kv : W->ctx.timings)
+                if (kv.second.second >= 0.5) ph += " " + kv.first + "=" + std::to_string(kv.second.second);
+            W->ctx.timings.clear();
+            std::fprintf(S->trace, "%d %d %llu %llu %.3f %.3f %.3f #%s\n", W->index,
+                         batch.empty() ? -1 : (batch[0].seq.size() <= kShortMax ? 0 : 1),
+                         static_cast<unsigned long long>(n), static_cast<unsigned long long>(bases),
+                         std::chrono::duration<double, std::milli>(tb0 - S->t_create).count(),
+                         std::chrono::duration<double, std::milli>(tb1 - tb0).count(),
+                         std::chrono::duration<double, std::milli>(tb0 - oldest).count(), ph.c_str());
         }
-        S->cv_done.notify_all();
-        S->cv_work.notify_all();
+        finish_batch(S, W, batch, st, W->rr.as<phr_read_result>(), W->aln.as<phr_alignment>(), W->cig.as<char>());
     }
 }
 
@@ -163,34 +234,42 @@ uint64_t batch_need(uint64_t n, uint64_t bases) {
 void run_scheduler(phr_server* S) {
     cudaSetDevice(S->owner->device);
     std::unique_lock<std::mutex> lk(S->mu);
+    // bucket an idle worker can take now: -1 none
+    auto pick = [&](const phr_server::Worker* w) -> int {
+        const bool s0 = !S->pending[0].empty(), s1 = !S->pending[1].empty();
+        if (w->short_only) return s0 ? 0 : -1;
+        if (s0 && s1) return S->pending[1].front().t0 < S->pending[0].front().t0 ? 1 : 0;
+        if (s1) return 1;
+        // short reads go to a general worker only while the short lane is busy
+        if (s0 && S->short_lane && !S->workers[0]->busy) return -1;
+        return s0 ? 0 : -1;
+    };
+    auto ready = [&]() -> bool {
+        for (auto* w : S->workers)
+            if (!w->busy && pick(w) >= 0) return true;
+        return false;
+    };
     for (;;) {
         S->cv_work.wait(lk, [&] {
-            return S->stopping || ((!S->pending[0].empty() || !S->pending[1].empty()) &&
-                                   std::any_of(S->workers.begin(), S->workers.end(), [](auto* w) { return !w->busy; }));
+            return ready() || (S->stopping && S->pending[0].empty() && S->pending[1].empty());
         });
-        const bool have = !S->pending[0].empty() || !S->pending[1].empty();
-        if (!have && S->stopping) {
+        if (S->stopping && S->pending[0].empty() && S->pending[1].empty()) {
             for (auto* w : S->workers) w->cv.notify_all();
             return;
         }
-        if (!have) continue;
-        // oldest request decides the bucket
-        int b = 0;
-        if (S->pending[0].empty()) b = 1;
-        else if (!S->pending[1].empty() && S->pending[1].front().t0 < S->pending[0].front().t0) b = 1;
-        // batch-forming window: give late arrivals max_wait_us to join a partial batch
-        const auto deadline = S->pending[b].front().t0 + std::chrono::microseconds(S->cfg.max_wait_us);
-        while (!S->stopping && S->pending[b].size() < S->cfg.max_batch_reads && Clock::now() < deadline) {
-            S->cv_work.wait_until(lk, deadline);
-        }
-        if (S->pending[b].empty()) continue;
         phr_server::Worker* W = nullptr;
+        int b = -1;
         for (auto* w : S->workers)
-            if (!w->busy) {
+            if (!w->busy && (b = pick(w)) >= 0) {
                 W = w;
                 break;
             }
         if (!W) continue;
+        // batch-forming window: give late arrivals max_wait_us to join a partial batch
+        const auto deadline = S->pending[b].front().t0 + std::chrono::microseconds(S->cfg.max_wait_us);
+        while (!S->stopping && S->pending[b].size() < S->cfg.max_batch_reads && Clock::now() < deadline)
+            S->cv_work.wait_until(lk, deadline);
+        if (S->pending[b].empty() || W->busy) continue;
         std::vector<Request> batch;
         uint64_t bases = 0;
         while (!S->pending[b].empty() && batch.size() < S->cfg.max_batch_reads) {
@@ -222,6 +301,16 @@ void run_scheduler(phr_server* S) {
     }
 }
 
+void enqueue_locked(phr_server* S, const uint8_t* read, uint32_t len, Clock::time_point t0, uint64_t* id) {
+    Request r;
+    r.seq.assign(read, read + len);
+    r.t0 = t0;
+    r.id = S->next_id++;
+    *id = r.id;
+    S->pending[len <= kShortMax ? 0 : 1].push_back(std::move(r));
+    S->in_flight += 1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -241,21 +330,59 @@ phr_status phr_server_create(phr_ctx* c, const phr_index* idx, const phr_server_
         delete S;
         return PHR_ERR_ARG;
     }
+    S->short_lane = S->cfg.short_lane > 0 || (S->cfg.short_lane == 0 && S->cfg.n_streams >= 2);
+    if (S->cfg.long_blocks_per_sm == 0) S->cfg.long_blocks_per_sm = 2;
+    if (S->cfg.long_blocks_per_sm > 4) {
+        delete S;
+        return PHR_ERR_ARG;
+    }
+    int prio_low = 0, prio_high = 0;
+    cudaSetDevice(c->impl.device);
+    cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     for (uint32_t w = 0; w < S->cfg.n_streams; ++w) {
         auto* W = new phr_server::Worker();
         W->ctx.device = c->impl.device;
         W->ctx.sm_count = c->impl.sm_count;
         W->ctx.tune = c->impl.tune;
         W->ctx.scratch_budget = c->impl.scratch_budget;
-        cudaSetDevice(W->ctx.device);
-        if (cudaStreamCreateWithFlags(&W->ctx.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        W->short_only = S->short_lane && w == 0;
+        W->index = static_cast<int>(w);
+        if (S->short_lane && w > 0)
+            W->ctx.tune.max_blocks_per_sm = std::min<int>(W->ctx.tune.max_blocks_per_sm,
+                                                          static_cast<int>(S->cfg.long_blocks_per_sm));
+        const int prio = W->short_only ? prio_high : prio_low;
+        if (cudaStreamCreateWithPriority(&W->ctx.stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
             delete W;
             for (auto* x : S->workers) delete x;
             delete S;
             return PHR_ERR_CUDA;
         }
+        W->ctx.bind_stream();
+        W->ctx.timing = std::getenv("PHRAYA_SERVER_TRACE") != nullptr;
+        // Device arenas and host buffers for a full batch up front: growing them while
+        // serving (allocation, page-locking) stalls every worker on the device.
+        {
+            const uint64_t nr = S->cfg.max_batch_reads;
+            const uint64_t nb = W->short_only ? std::min<uint64_t>(S->cfg.max_batch_bases, nr * kShortMax)
+                                              : S->cfg.max_batch_bases;
+            W->ctx.pipe.reserve(phr::align_arena_need(nr, nb, 0) + nb + nr * 32);
+            W->ctx.seeds.reserve(nb * 40 + (16ull << 20));
+            W->ctx.io.reserve(nb * 16 + nr * 1024 + (16ull << 20));
+            W->ctx.arena.reserve(nb * 24 + nr * 2048 + (96ull << 20));
+            W->ctx.scratch.reserve(std::min<uint64_t>(W->ctx.scratch_budget, W->short_only ? (512ull << 20) : (4ull << 30)));
+            cudaGetLastError();
+            const uint32_t K = S->cfg.align.strategy == PHR_FAST ? 1 : S->cfg.align.strategy == PHR_BALANCED ? 2 : 50;
+            W->seq.ensure(nb + 64);
+            W->off.ensure(nr * 8);
+            W->len.ensure(nr * 4);
+            W->rr.ensure(nr * sizeof(phr_read_result));
+            W->aln.ensure((nr * K + 16) * sizeof(phr_alignment));
+            W->cig.ensure(std::min<uint64_t>(K * (6 * nb + 16 * nr) + 64, 256ull << 20));
+        }
         S->workers.push_back(W);
     }
+    S->t_create = Clock::now();
+    if (const char* tp = std::getenv("PHRAYA_SERVER_TRACE")) S->trace = std::fopen(tp, "w");
     for (auto* W : S->workers) W->th = std::thread(run_worker, S, W);
     S->scheduler = std::thread(run_scheduler, S);
     *out = S;
@@ -264,17 +391,26 @@ phr_status phr_server_create(phr_ctx* c, const phr_index* idx, const phr_server_
 
 phr_status phr_server_submit(phr_server* S, const uint8_t* read, uint32_t len, uint64_t* request_id) {
     if (!S || (!read && len) || !request_id) return PHR_ERR_ARG;
-    Request r;
-    r.seq.assign(read, read + len);
-    r.t0 = Clock::now();
+    const auto t0 = Clock::now();
     {
         std::lock_guard<std::mutex> lk(S->mu);
         if (S->stopping) return PHR_ERR_STATE;
         if (S->fatal != PHR_OK) return S->fatal;
-        r.id = S->next_id++;
-        *request_id = r.id;
-        S->pending[len <= kShortMax ? 0 : 1].push_back(std::move(r));
-        S->in_flight += 1;
+        enqueue_locked(S, read, len, t0, request_id);
+    }
+    S->cv_work.notify_all();
+    return PHR_OK;
+}
+
+phr_status phr_server_submit_many(phr_server* S, const uint8_t* seq, const uint64_t* off, const uint32_t* len,
+                                  uint64_t n, uint64_t* ids) {
+    if (!S || (n && (!seq || !off || !len || !ids))) return PHR_ERR_ARG;
+    const auto t0 = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stopping) return PHR_ERR_STATE;
+        if (S->fatal != PHR_OK) return S->fatal;
+        for (uint64_t i = 0; i < n; ++i) enqueue_locked(S, seq + off[i], len[i], t0, ids + i);
     }
     S->cv_work.notify_all();
     return PHR_OK;
@@ -326,6 +462,7 @@ phr_status phr_server_destroy(phr_server* S) {
         if (W->th.joinable()) W->th.join();
     }
     const phr_status st = S->fatal;
+    if (S->trace) std::fclose(S->trace);
     for (auto* W : S->workers) {
         cudaSetDevice(W->ctx.device);
         cudaStreamSynchronize(W->ctx.stream);

@@ -48,3 +48,27 @@ def test_alone_equals_mixed_equals_batched(strat):
     assert mixed == batched
     lat = [got[i][1] for i in ids]
     assert min(lat) > 0
+
+
+@pytest.mark.parametrize("short_lane", [1, -1])
+def test_submit_many_and_lanes(short_lane):
+    """Batched submission and both lane layouts return the batched call's results; long
+    reads (one-CTA-per-pair WFA path) and short reads share the stream."""
+    eng = P.Engine(0)
+    ref = D.random_reference(400_000, seed=44)
+    idx = eng.index(ref)
+    short, _, _ = D.reads_on_reference(ref, 300, 150, 0.01, seed=45)
+    longr, _, _ = D.reads_on_reference(ref, 12, 5000, 0.05, seed=46)
+    reads = [bytes(short.seq[o:o + l]) for o, l in zip(short.off, short.len)]
+    reads += [bytes(longr.seq[o:o + l]) for o, l in zip(longr.off, longr.len)]
+    reads = [reads[i] for i in sorted(range(len(reads)), key=lambda i: (i * 7919) % len(reads))]
+    batched, _ = eng.align_reads(idx, reads, A.BALANCED)
+    srv = eng.server(idx, strategy=A.BALANCED, max_batch_reads=128, max_wait_us=300, n_streams=3,
+                     short_lane=short_lane, long_blocks_per_sm=1)
+    ids = []
+    for k in range(0, len(reads), 50):
+        ids += srv.submit_many(reads[k:k + 50])
+    assert len(set(ids)) == len(reads)
+    got = drain(srv, len(reads))
+    srv.close()
+    assert [got[i][0] for i in ids] == batched
