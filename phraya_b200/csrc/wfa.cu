@@ -942,7 +942,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
 
 // Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
 template <class S, bool kAffine>
-__global__ void __launch_bounds__(256) wfa_kernel(ExtendParams P) {
+__global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams P) {
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     for (;;) {
