@@ -167,6 +167,7 @@ def run_engine(args, rank, world):
 
     from phraya_b200 import _abi as A
     from phraya_b200 import api as P
+    from phraya_b200 import dist as R
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -211,8 +212,7 @@ def run_engine(args, rank, world):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    R.barrier()
     L.phr_ctx_reset_timing(eng.handle)
     L.phr_ctx_set_timing(eng.handle, 1)
     launches0 = eng.kernel_launches
@@ -229,11 +229,7 @@ def run_engine(args, rank, world):
     clk = clocks.stop()
     L.phr_ctx_set_timing(eng.handle, 0)
     launches = eng.kernel_launches - launches0
-    elapsed_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([elapsed_ms], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = R.max_over_ranks(e0.elapsed_time(e1), device=f"cuda:{dev}")
     ms_per_step = elapsed_ms / args.steps
     per_step_pairs = 2 * n_a + n_b
     value = per_step_pairs * world / (ms_per_step / 1000.0)
@@ -281,19 +277,19 @@ def run_engine(args, rank, world):
             eng.check(L.phr_extend_batch(eng.handle, eng_id, C.byref(b), A.AffineCosts(*costs), C.byref(arena)))
             d2h += p.n * C.sizeof(A.Alignment) + arena.cigar_used
 
-    e2e_step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(max(1, args.warmup)):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    R.barrier()
+    # CUDA events on the context stream: the host copies of phr_extend_batch run on it
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = R.max_over_ranks(f0.elapsed_time(f1) / 1000.0 / args.steps, device=f"cuda:{dev}")
     h2d = 2 * input_bytes(set_a) + input_bytes(set_b)
 
     if rank != 0:
@@ -322,8 +318,17 @@ def run_engine(args, rank, world):
         ops = dp_cells(set_a)
         work = "DP-equivalent cells of set A per step"
     achieved = ops / (step_ms / 1000.0) / 1e12
+    # DRAM bytes per step of the dominant kernel: ncu dram__bytes_read.sum + write.sum of
+    # myers_kernel on 100,000 pairs of the same distribution (9.95 GB), scaled by the pair
+    # count (profiles/myers_kernel_set_b_100k.md); None for another dominant kernel
+    traffic, traffic_src = None, None
+    if args.traffic_gb_per_step is not None:
+        traffic, traffic_src = args.traffic_gb_per_step * 1e9, "--traffic-gb-per-step"
+    elif name.startswith("myers"):
+        traffic = 9.95e9 * n_b / 100000
+        traffic_src = "ncu capture of 100,000 pairs (9.95 GB), scaled by pairs"
     roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tops/s",
-            "frac": achieved / int_peak_tops, "traffic": args.traffic_gb_per_step, "kernel": name,
+            "frac": achieved / int_peak_tops, "traffic": traffic, "traffic_source": traffic_src, "kernel": name,
             "kernel_ms_per_step": step_ms, "launches_per_step": nl / args.steps, "work": work,
             "peak_source": "nominal integer issue rate 148 SMs x 4 x 32 lanes x max SM clock "
                            f"({peaks.get('sm_max_mhz', 1965.0)} MHz, {peak_src}); no measured integer peak exists"}
