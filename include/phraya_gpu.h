@@ -122,8 +122,9 @@ phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out);
 void phr_ctx_destroy(phr_ctx* ctx);
 /* Launch parameters of the extension kernels. No counterpart in the reference (its
  * kernels are CPU code with nothing to tune); results never depend on them. Keys:
- *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen 1024
- *                                        (power of two, 1..32)
+ *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen
+ *                                        wfa_long_min (power of two, 1..32)
+ *   "wfa_long_min"                       that length-bucket edge (default 1024)
  *   "myers_band_base"                    Myers stored-band half-width base (>= 0)
  *   "block_threads"                      threads per block of the warp-per-pair kernels
  *                                        (32..256, multiple of 32)

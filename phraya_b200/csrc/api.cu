@@ -158,6 +158,7 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "wfa_big_min")) return &t.wfa_big_min;
     if (!std::strcmp(key, "wfa_big_smem")) return &t.wfa_big_smem;
     if (!std::strcmp(key, "max_blocks_per_sm")) return &t.max_blocks_per_sm;
+    if (!std::strcmp(key, "wfa_long_min")) return &t.wfa_long_min;
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
@@ -168,6 +169,7 @@ bool tune_valid(const char* key, int64_t v) {
     if (!std::strcmp(key, "wfa_big_min")) return v >= 0 && v <= INT32_MAX;
     if (!std::strcmp(key, "wfa_big_smem")) return v >= (16 << 10) && v <= (200 << 10) && v % 16 == 0;
     if (!std::strcmp(key, "max_blocks_per_sm")) return v >= 1 && v <= 4;
+    if (!std::strcmp(key, "wfa_long_min")) return v >= 0 && v <= INT32_MAX;
     return false;
 }
 }  // namespace

@@ -204,6 +204,7 @@ struct PackParams {
     uint32_t* keys;
     uint32_t* vals;
     int wfa_g_short, wfa_g_long;
+    int wfa_long_min;   // qn + tn from which a WFA pair gets wfa_g_long lanes
 };
 
 // 2-bit packing (16 bases per word) of both suffixes; a pair holding any byte other
@@ -307,7 +308,7 @@ __global__ void pack_kernel(PackParams P) {
             G = next_pow2_cap32((d.qn + 63) / 64);
             len = static_cast<uint32_t>(d.tn) * (static_cast<uint32_t>((d.qn + 63) / 64));
         } else {
-            G = (d.qn + d.tn < 1024) ? P.wfa_g_short : P.wfa_g_long;
+            G = (d.qn + d.tn < P.wfa_long_min) ? P.wfa_g_short : P.wfa_g_long;
             len = static_cast<uint32_t>(d.qn + d.tn);
         }
         const uint32_t glog = static_cast<uint32_t>(__ffs(G) - 1);
@@ -408,7 +409,7 @@ __global__ void task_finalize_kernel(TaskBuild T) {
 
 // Redo pass task list: one pair per task, in redo order.
 __global__ void redo_tasks_kernel(const uint32_t* redo_list, const uint32_t* redo_count, const PairDesc* desc,
-                                  int32_t engine, int wfa_g_short, int wfa_g_long, int32_t big_min,
+                                  int32_t engine, int wfa_g_short, int wfa_g_long, int wfa_long_min, int32_t big_min,
                                   uint32_t big_smem, uint32_t* task_first, uint8_t* task_count,
                                   uint8_t* task_group, uint32_t* ranges) {
     const uint32_t n = *redo_count;
@@ -423,7 +424,7 @@ __global__ void redo_tasks_kernel(const uint32_t* redo_list, const uint32_t* red
     if (engine == PHR_ENGINE_MYERS_FIT || engine == PHR_ENGINE_MYERS_GLOBAL)
         G = next_pow2_cap32((d.qn + 63) / 64);
     else
-        G = (d.qn + d.tn < 1024) ? wfa_g_short : wfa_g_long;
+        G = (d.qn + d.tn < wfa_long_min) ? wfa_g_short : wfa_g_long;
     task_first[t] = t;
     task_count[t] = 1;
     task_group[t] = static_cast<uint8_t>(G);
@@ -600,7 +601,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     cub::DeviceScan::ExclusiveSum(tmp, tn_, tb, tbo, static_cast<int>(n), st);
 
     PackParams pk{in, engine, costs, desc, pout, w2o, wbo, tbo, arena2, arenab, text, keys, vals,
-                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long};
+                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long, ctx->tune.wfa_long_min};
     {
         KernelScope ks(ctx, "pack");
         pack_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(pk);
@@ -814,6 +815,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                 KernelScope ks(ctx, "redo_tasks");
                 redo_tasks_kernel<<<blocks_for(m, T), T, 0, st>>>(rlist2, cnt + 18, desc, engine,
                                                                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long,
+                                                                 ctx->tune.wfa_long_min,
                                                                  P.big_min, P.big_smem, task_first, task_count,
                                                                  task_group, cnt + 14);
             }

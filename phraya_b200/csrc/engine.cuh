@@ -35,6 +35,7 @@ struct DeviceArena {
 struct EngineTune {
     int wfa_group_short = 16;    // lanes per pair for WFA pairs with qn+tn < 1024
     int wfa_group_long = 32;
+    int wfa_long_min = 1024;     // bucket edge: qn+tn from which WFA pairs get wfa_group_long lanes
     int myers_band_base = 64;
     int block_threads = 256;
     int wfa_big_min = 4096;          // linear WFA pairs with qn+tn >= this run one per CTA (0: off)
