@@ -108,6 +108,48 @@ def input_bytes(p):
     return int(p.seq.nbytes + p.q_off.nbytes + p.q_len.nbytes + p.t_off.nbytes + p.t_len.nbytes)
 
 
+def packed_bytes(p):
+    """2-bit packed bytes of every query and target (16 bases per 32-bit word)."""
+    return 4.0 * float(((p.q_len.astype(np.int64) + 15) // 16).sum() + ((p.t_len.astype(np.int64) + 15) // 16).sum())
+
+
+def roofline(name, step_ms, launches, work, set_a, set_b, int_peak, hbm_peak, peak_src, traffic_gb=None):
+    """Roofline of one kernel over a step: algorithmic work from the kernel's own counters,
+    bound = the resource (integer issue or HBM) whose lower-bound time is longer."""
+    sec = step_ms / 1000.0
+    if name == "myers_lane":
+        cols = work["myers_lane_block_columns"]      # 64-row block x column steps evaluated
+        ops = cols * 64 * 22.0 / 32.0                # 22 word operations per 32 rows per column
+        # {VP, HP} records written (16 B per block-column), read back along the path
+        # (>= one 16 B record per target column), packed inputs
+        nbytes = cols * 16.0 + float(set_b.t_len.astype(np.float64).sum()) * 16.0 + packed_bytes(set_b)
+        t_int, t_hbm = ops / int_peak, nbytes / hbm_peak
+        work_txt = ("band cells = 64 x block-columns evaluated (kernel counter); int ops = cells x 22/32; "
+                    "bytes = 16 B {VP,HP} record per block-column + 16 B read back per target column + 2-bit inputs")
+    else:
+        return {"kernel": name, "kernel_ms_per_step": step_ms, "bound": None,
+                "note": "no work counter for this kernel"}
+    if t_hbm >= t_int:
+        bound, achieved, peak, unit = "hbm", nbytes / sec / 1e9, hbm_peak / 1e9, "GB/s"
+        psrc = f"measured copy bandwidth ({peak_src})"
+    else:
+        bound, achieved, peak, unit = "int", ops / sec / 1e12, int_peak / 1e12, "Tops/s"
+        psrc = "nominal integer issue rate 148 SMs x 4 x 32 lanes x max SM clock"
+    traffic, traffic_src = None, None
+    if traffic_gb is not None:
+        traffic, traffic_src = traffic_gb * 1e9, "--traffic-gb-per-step"
+    elif name == "myers_lane":
+        # ncu dram__bytes_read.sum + write.sum of one launch on 100,000 pairs of the same
+        # distribution (6.34 GB), scaled by the pair count
+        traffic = 6.34e9 * set_b.n / 100000
+        traffic_src = "ncu capture of 100,000 pairs (6.34 GB), scaled by pairs"
+    return {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
+            "traffic": traffic, "traffic_source": traffic_src, "kernel": name, "kernel_ms_per_step": step_ms,
+            "launches_per_step": launches, "work": work_txt, "peak_source": psrc,
+            "int_frac": ops / sec / int_peak, "hbm_frac": nbytes / sec / hbm_peak,
+            "band_cells_per_step": cols * 64, "redo_pairs_per_step": work["myers_lane_redo_pairs"]}
+
+
 def cpu_baseline(set_a, set_b, n_a, n_b, nthreads, sample_a=60000, sample_b=6000):
     """Times the oracle (CPU restatement) on a bounded sample and scales to the job."""
     import oracle as O
@@ -241,6 +283,8 @@ def run_engine(args, rank, world):
     nrec = L.phr_ctx_get_timing(eng.handle, recs, 64)
     ktimes = {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(min(nrec, 64))
               if not recs[i].name.startswith(b"host:")}
+    # work counters of the timed steps (reset with the timings)
+    work = {k: eng.counter(k) / args.steps for k in ("myers_lane_block_columns", "myers_lane_redo_pairs")}
 
     # ---- end to end through the host API, pinned host buffers ----------------
     def pinned_pairs(p):
@@ -296,42 +340,13 @@ def run_engine(args, rank, world):
         return
     # ---- roofline of the dominant kernel (its device time per step, CUDA events) ----
     peaks, peak_src = load_peaks()
-    # kernel families: main pass, byte-mode instantiation and redo passes of one engine
-    fam = {}
-    for k, (nlk, totk) in ktimes.items():
-        if k.startswith("host:"):
-            continue
-        f = next((p for p in ("myers", "wfa_affine", "wfa_linear") if k.startswith(p)), k)
-        a = fam.setdefault(f, [0, 0.0])
-        a[0] += nlk
-        a[1] += totk
-    name, (nl, tot) = max(fam.items(), key=lambda kv: kv[1][1])
-    step_ms = tot / args.steps           # all launches of that kernel family in one step
-    int_peak_tops = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    if name.startswith("myers"):
-        ops = dp_cells(set_b) * 22.0 / 32.0
-        work = "sum(m*n) * 22/32 integer ops per step (set B, all launches incl. band redo)"
-    elif name.startswith("wfa_affine"):
-        ops = dp_cells(set_a)
-        work = "DP-equivalent cells of set A per step"
-    else:
-        ops = dp_cells(set_a)
-        work = "DP-equivalent cells of set A per step"
-    achieved = ops / (step_ms / 1000.0) / 1e12
-    # DRAM bytes per step of the dominant kernel: ncu dram__bytes_read.sum + write.sum of
-    # myers_kernel on 100,000 pairs of the same distribution (9.95 GB), scaled by the pair
-    # count (profiles/myers_kernel_set_b_100k.md); None for another dominant kernel
-    traffic, traffic_src = None, None
-    if args.traffic_gb_per_step is not None:
-        traffic, traffic_src = args.traffic_gb_per_step * 1e9, "--traffic-gb-per-step"
-    elif name.startswith("myers"):
-        traffic = 9.95e9 * n_b / 100000
-        traffic_src = "ncu capture of 100,000 pairs (9.95 GB), scaled by pairs"
-    roof = {"bound": "int", "achieved": achieved, "peak": int_peak_tops, "unit": "Tops/s",
-            "frac": achieved / int_peak_tops, "traffic": traffic, "traffic_source": traffic_src, "kernel": name,
-            "kernel_ms_per_step": step_ms, "launches_per_step": nl / args.steps, "work": work,
-            "peak_source": "nominal integer issue rate 148 SMs x 4 x 32 lanes x max SM clock "
-                           f"({peaks.get('sm_max_mhz', 1965.0)} MHz, {peak_src}); no measured integer peak exists"}
+    kms = {k: tot / args.steps for k, (_nl, tot) in ktimes.items()}
+    name = max(kms, key=kms.get)
+    step_ms = kms[name]
+    int_peak = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6   # ops/s, nominal issue
+    hbm_peak = peaks.get("hbm_gbs", 6650.0) * 1e9                      # bytes/s, measured copy
+    roof = roofline(name, step_ms, ktimes[name][0] / args.steps, work, set_a, set_b, int_peak, hbm_peak,
+                    peak_src, args.traffic_gb_per_step)
     pipe = None
     if not args.no_pipeline:
         pipe = run_pipeline(eng, dev, args)

@@ -109,7 +109,8 @@ typedef struct {
 typedef struct phr_ctx phr_ctx;
 
 typedef struct {
-    uint64_t workspace_bytes;  /* cap on extension scratch; 0 = default (8 GiB)         */
+    uint64_t workspace_bytes;  /* cap on extension scratch; 0 = default (a fifth of the
+                                  device memory, within 8 GiB .. 48 GiB)                */
     int32_t tune_file_enable;  /* 1 = read/write autotuner cache file                   */
     const char* tune_file;     /* NULL = "phraya_b200_tune.txt" in the working dir      */
 } phr_config;
@@ -156,7 +157,15 @@ typedef struct {
 phr_status phr_ctx_set_timing(phr_ctx* ctx, int32_t enable);
 /* Copies up to `max` per-kernel records; returns how many kernels have records. */
 uint32_t phr_ctx_get_timing(const phr_ctx* ctx, phr_kernel_timing* out, uint32_t max);
+/* Clears the kernel times and the work counters below. */
 void phr_ctx_reset_timing(phr_ctx* ctx);
+/*
+ * Work counters accumulated over the context's extension calls (no counterpart in the
+ * reference): "myers_lane_block_columns" counts the 64-row block x column steps the
+ * banded Myers kernel evaluated (64 DP cells each); "myers_lane_redo_pairs" the pairs
+ * it handed to the every-block redo pass. Unknown names read 0.
+ */
+uint64_t phr_ctx_counter(const phr_ctx* ctx, const char* name);
 /* The cudaStream_t the context launches on (for callers that order their own work). */
 void* phr_ctx_stream(const phr_ctx* ctx);
 

@@ -241,6 +241,7 @@ PROTOTYPES = {
     "phr_ctx_get_tune": (C.c_int32, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
     "phr_ctx_get_timing": (C.c_uint32, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "phr_ctx_reset_timing": (None, [C.c_void_p]),
+    "phr_ctx_counter": (C.c_uint64, [C.c_void_p, C.c_char_p]),
     "phr_ctx_stream": (C.c_void_p, [C.c_void_p]),
     "phr_extend_batch": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(PairBatch), AffineCosts,
                                      C.POINTER(ResultArena)]),

@@ -135,6 +135,20 @@ class Engine:
     def kernel_launches(self):
         return int(self._lib.phr_ctx_kernel_launches(self._h))
 
+    def set_timing(self, enable=True):
+        """Times every kernel launch with CUDA events (phr_ctx_set_timing)."""
+        self.check(self._lib.phr_ctx_set_timing(self._h, 1 if enable else 0))
+
+    def counter(self, name):
+        """Work counter of the context (phr_ctx_counter), e.g. "myers_lane_block_columns"."""
+        return int(self._lib.phr_ctx_counter(self._h, name.encode()))
+
+    def kernel_times(self):
+        """{kernel name: (launches, total ms)} recorded while timing was on."""
+        recs = (A.KernelTiming * 64)()
+        n = int(self._lib.phr_ctx_get_timing(self._h, recs, 64))
+        return {recs[i].name.decode(): (int(recs[i].launches), float(recs[i].total_ms)) for i in range(min(n, 64))}
+
     # -- pairs API ----------------------------------------------------------
     def extend_packed(self, engine, packed, costs=AffineCosts(), percall=False):
         """Runs one engine over a PackedPairs batch; returns (aln ndarray, cigar bytes)."""

@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libphraya_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["engine.cu", "myers.cu", "wfa.cu", "api.cu", "pipeline.cu", "server.cu"]
+SOURCES = ["engine.cu", "myers.cu", "myers_lane.cu", "wfa.cu", "api.cu", "pipeline.cu", "server.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

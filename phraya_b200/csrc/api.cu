@@ -134,6 +134,13 @@ phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out) 
         return PHR_ERR_CUDA;
     }
     ctx->bind_stream();
+    {
+        // default scratch cap: a fifth of the device memory, within [8 GiB, 48 GiB]
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+            ctx->scratch_budget = std::min<size_t>(std::max<size_t>(tot / 5, 8ull << 30), 48ull << 30);
+        cudaGetLastError();
+    }
     if (cfg && cfg->workspace_bytes) ctx->scratch_budget = cfg->workspace_bytes;
     if (cfg && cfg->tune_file_enable) {
         ctx->tune_file_enable = true;
@@ -225,6 +232,15 @@ void phr_ctx_reset_timing(phr_ctx* c) {
     if (!c) return;
     std::lock_guard<std::mutex> lk(c->impl.mu);
     c->impl.timings.clear();
+    c->impl.counters.clear();
+}
+
+uint64_t phr_ctx_counter(const phr_ctx* c, const char* name) {
+    if (!c || !name) return 0;
+    phr_ctx* m = const_cast<phr_ctx*>(c);
+    std::lock_guard<std::mutex> lk(m->impl.mu);
+    auto it = m->impl.counters.find(name);
+    return it == m->impl.counters.end() ? 0 : it->second;
 }
 
 void* phr_ctx_stream(const phr_ctx* c) { return c ? static_cast<void*>(c->impl.stream) : nullptr; }

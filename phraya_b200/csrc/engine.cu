@@ -205,6 +205,7 @@ struct PackParams {
     uint32_t* vals;
     int wfa_g_short, wfa_g_long;
     int wfa_long_min;   // qn + tn from which a WFA pair gets wfa_g_long lanes
+    int band_base;      // Myers band half-width base
 };
 
 // 2-bit packing (16 bases per word) of both suffixes; a pair holding any byte other
@@ -306,6 +307,11 @@ __global__ void pack_kernel(PackParams P) {
         uint32_t len;
         if (P.engine == PHR_ENGINE_MYERS_FIT || P.engine == PHR_ENGINE_MYERS_GLOBAL) {
             G = next_pow2_cap32((d.qn + 63) / 64);
+            // global 2-bit pairs whose band fits the lane kernel's window: one lane each
+            if (P.engine == PHR_ENGINE_MYERS_GLOBAL && d.mode == 0) {
+                const LaneBand b = lane_band(d.qn, d.tn, P.band_base);
+                if (lane_slots(b.dmin, b.dmax, (d.qn + 63) / 64) <= kLaneMaxSlots - 2) G = 1;
+            }
             len = static_cast<uint32_t>(d.tn) * (static_cast<uint32_t>((d.qn + 63) / 64));
         } else {
             G = (d.qn + d.tn < P.wfa_long_min) ? P.wfa_g_short : P.wfa_g_long;
@@ -330,6 +336,7 @@ struct TaskBuild {
     uint8_t* task_group;
     uint32_t* ranges;          // {0, split, split, n_tasks}
     uint32_t* split_min;
+    uint32_t* g1_min;          // first 2-bit task of more than one lane per pair
     const PairDesc* desc;
     int32_t engine;
     int32_t band_base;
@@ -376,17 +383,27 @@ __global__ void task_fill_kernel(TaskBuild T) {
     const uint32_t per = 32 / G;
     uint32_t cnt = 0;
     uint64_t need = 0, region = 0;
+    // lane-kernel tasks (global Myers, 2-bit, one lane per pair): window over the union band
+    const bool lane_task = T.engine == PHR_ENGINE_MYERS_GLOBAL && G == 1 && !((k >> 31) & 1);
+    int dmin = 0x7fffffff, dmax = static_cast<int>(0x80000000), n_max = 0, m_max = 0;
     for (uint32_t c = 0; c < per && p + c < T.n; ++c) {
         const uint32_t kc = T.keys[p + c];
         if (kc == kInvalidKey || key_seg(kc) != key_seg(k)) break;
         const PairDesc d = T.desc[T.order[p + c]];
-        if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
+        if (lane_task) {
+            const LaneBand b = lane_band(d.qn, d.tn, T.band_base);
+            dmin = min(dmin, b.dmin);
+            dmax = max(dmax, b.dmax);
+            n_max = max(n_max, d.tn);
+            m_max = max(m_max, d.qn);
+        } else if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
             need += myers_need_est(d.qn, d.tn, G, T.band_base);
         else if (!big_pair(T.engine, T.big_min, T.big_smem, d.qn, d.tn, d.mode))
             region = max(region, wfa_region_est(d.qn, d.tn, T.engine == PHR_ENGINE_WFA_AFFINE));
         ++cnt;
     }
     if (T.engine != PHR_ENGINE_MYERS_FIT && T.engine != PHR_ENGINE_MYERS_GLOBAL) need = region * per;
+    if (lane_task && cnt) need = lane_task_need(n_max, m_max, lane_slots(dmin, dmax, (m_max + 63) >> 6));
     const uint32_t t = T.tidx[p];
     T.task_first[t] = static_cast<uint32_t>(p);
     T.task_count[t] = static_cast<uint8_t>(cnt);
@@ -395,6 +412,7 @@ __global__ void task_fill_kernel(TaskBuild T) {
     if (need) atomicAdd(&T.need_hist[64 - __clzll(need)], 1u);
     atomicMax(T.need_max, static_cast<unsigned long long>(need));
     if ((k >> 31) & 1) atomicMin(T.split_min, t);
+    else if (G > 1) atomicMin(T.g1_min, t);
 }
 
 __global__ void task_finalize_kernel(TaskBuild T) {
@@ -405,6 +423,12 @@ __global__ void task_finalize_kernel(TaskBuild T) {
     T.ranges[1] = split;
     T.ranges[2] = split;
     T.ranges[3] = nt;
+    // lane-kernel range {0, g1} and warp-group 2-bit range {g1, split} (global Myers)
+    const uint32_t g1 = min(*T.g1_min, split);
+    T.ranges[28] = 0;
+    T.ranges[29] = g1;
+    T.ranges[30] = g1;
+    T.ranges[31] = split;
 }
 
 // Redo pass task list: one pair per task, in redo order.
@@ -568,13 +592,16 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     uint64_t* rtask_len = static_cast<uint64_t*>(take(n * 8));
     unsigned int* need_hist = static_cast<unsigned int*>(take(64 * 4));
     // counters: [0..3] ranges, [4] split_min, [5] queue head 0, [6] queue head 1,
-    // [7] redo count, [8..9] need max (u64), [10] error flag, [12..13] total (u64), [14..17] redo ranges
+    // [7] redo count, [8..9] need max (u64), [10] error flag, [12..13] total (u64), [14..17] redo ranges,
+    // [20] first multi-lane 2-bit task, [24..25] CTA-kernel queue heads, [26] lane-kernel queue head,
+    // [28..31] lane-kernel and warp-group 2-bit ranges (global Myers), [32..35] work counters (u64)
     uint32_t* cnt = static_cast<uint32_t*>(take(256));
     if (!cnt) return set_error(ctx, PHR_ERR_OOM, "device arena exhausted");
     unsigned long long* need_max = reinterpret_cast<unsigned long long*>(cnt + 8);
     uint64_t* total = reinterpret_cast<uint64_t*>(cnt + 12);
     PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, 256, st));
     PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 4, 0xFF, 4, st));
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 20, 0xFF, 4, st));
 
     // CUB temp sizes
     size_t t_sort = 0, t_scan = 0, t_max = 0;
@@ -601,7 +628,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     cub::DeviceScan::ExclusiveSum(tmp, tn_, tb, tbo, static_cast<int>(n), st);
 
     PackParams pk{in, engine, costs, desc, pout, w2o, wbo, tbo, arena2, arenab, text, keys, vals,
-                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long, ctx->tune.wfa_long_min};
+                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long, ctx->tune.wfa_long_min,
+                  ctx->tune.myers_band_base};
     {
         KernelScope ks(ctx, "pack");
         pack_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(pk);
@@ -610,7 +638,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     cub::DeviceRadixSort::SortPairs(tmp, tn_, keys, keys_s, vals, order, static_cast<int>(n), 0, 32, st);
 
     PHR_CUDA_TRY(ctx, cudaMemsetAsync(need_hist, 0, 64 * 4, st));
-    TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, desc,
+    TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, cnt + 20, desc,
                   engine, ctx->tune.myers_band_base, need_max, task_need, need_hist,
                   ctx->tune.wfa_big_min, static_cast<uint32_t>(ctx->tune.wfa_big_smem)};
     {
@@ -683,6 +711,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     P.error_flag = cnt + 10;
     P.big_min = ctx->tune.wfa_big_min;
     P.big_smem = static_cast<uint32_t>(ctx->tune.wfa_big_smem);
+    P.work = reinterpret_cast<unsigned long long*>(cnt + 32);
 
     const int block = ctx->tune.block_threads;
     // main pass (per_task false): per-warp slots of `slot` bytes; redo passes: per-task
@@ -696,7 +725,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         uint64_t grid = static_cast<uint64_t>(ctx->sm_count) * ctx->tune.max_blocks_per_sm;
         if (!per_task) {
             slot = std::max<uint64_t>((slot + 255) & ~255ull, 4096);
-            // grid: resident blocks per SM, shrunk to the scratch budget
+            // grid: resident blocks per SM, no more warps than tasks, shrunk to the scratch budget
+            grid = std::max<uint64_t>(1, std::min<uint64_t>(grid, (h_ranges[3] + warps_per_block - 1) / warps_per_block));
             while (grid > 1 && grid * warps_per_block * slot > ctx->scratch_budget) grid = (grid + 1) / 2;
             PHR_CUDA_TRY(ctx, ctx->scratch.reserve(grid * warps_per_block * slot));
         } else {
@@ -718,6 +748,20 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         const int ek = is_myers ? 0 : engine == PHR_ENGINE_WFA_LINEAR ? 1 : 2;
         const char* kname = names[per_task][ek][0];
         const char* kname_b = names[per_task][ek][1];
+        if (!per_task && engine == PHR_ENGINE_MYERS_GLOBAL) {
+            // global 2-bit pairs of one lane each (tasks [0, g1)); the warp-group kernel
+            // below takes the remaining 2-bit tasks [g1, split)
+            const uint64_t lane_grid = std::min<uint64_t>(grid * warps_per_block / (kLaneThreads / 32),
+                                                          static_cast<uint64_t>(ctx->sm_count) * 2);
+            PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 26, 0, 4, st));
+            P.tasks.range = cnt + 28;
+            P.queue_head = cnt + 26;
+            {
+                KernelScope ks(ctx, "myers_lane");
+                launch_myers_lane(P, static_cast<int>(std::max<uint64_t>(lane_grid, 1)), st);
+            }
+            range0 = cnt + 30;
+        }
         P.tasks.range = range0;
         P.queue_head = cnt + 5;
         {
@@ -856,8 +900,12 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
     }
     uint32_t h_err = 0;
+    unsigned long long h_work[2] = {0, 0};
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_err, cnt + 10, 4, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_work, cnt + 32, sizeof(h_work), cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (h_work[0]) ctx->counters["myers_lane_block_columns"] += h_work[0];
+    if (h_work[1]) ctx->counters["myers_lane_redo_pairs"] += h_work[1];
     PHR_CUDA_TRY(ctx, cudaGetLastError());
     if (ctx->timing) ctx->resolve_timings();
     if (h_err) return set_error(ctx, PHR_ERR_CUDA, "internal consistency check failed (flags " + std::to_string(h_err) + ")");

@@ -69,6 +69,7 @@ struct Ctx {
     };
     std::vector<Pending> pending;
     std::map<std::string, std::pair<uint64_t, double>> timings;
+    std::map<std::string, uint64_t> counters;   // work counters (phr_ctx_counter)
     void begin_kernel(const char* name, cudaEvent_t* a);
     void end_kernel(const char* name, cudaEvent_t a);
     void resolve_timings();   // after a stream sync

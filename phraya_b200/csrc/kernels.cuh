@@ -41,6 +41,7 @@ struct ExtendParams {
     uint32_t* error_flag;       // set on an internal inconsistency (bounded loops ran out)
     int32_t big_min;            // linear WFA: pairs with qn+tn >= big_min run one per CTA (0: off)
     uint32_t big_smem;          // dynamic shared memory of the CTA-per-pair kernel (bytes)
+    unsigned long long* work;   // [0] banded Myers block-columns, [1] pairs sent to redo
 };
 
 // task_group bit marking a redo task for the CTA-per-pair kernel
@@ -74,7 +75,61 @@ __host__ __device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool
     return 16 * L + 4 * cells + 4096;
 }
 
+// ---------------------------------------------------------------------------
+// Lane-per-pair banded Myers (global mode, 2-bit pairs; myers_lane.cu).
+//
+// Band of one pair: every cell (i, j) of an alignment of cost ed satisfies
+// |i - j| + |(m - i) - (n - j)| <= ed, i.e. its diagonal d = j - i lies in
+// [min(0, n-m) - h, max(0, n-m) + h] with h = (ed - |n - m|) / 2. With E >= ed the
+// band is [dmin, dmax] below (one spare diagonal each side for the rounding of h).
+// A warp runs 32 pairs; its window covers the union of their bands and holds
+// P = ceil((dmax - dmin + 127) / 64) query blocks of 64 rows per column (at most nb).
+// ---------------------------------------------------------------------------
+constexpr int kLaneMaxSlots = 8;
+
+struct LaneBand {
+    int E;
+    int dmin, dmax;
+};
+
+__host__ __device__ __forceinline__ LaneBand lane_band(int m, int n, int band_base) {
+    const int delta = n - m;
+    const int ad = delta < 0 ? -delta : delta;
+    int E = band_base + ad + (m >> 4);
+    if (E > m + n) E = m + n;
+    const int h = (E - ad) >> 1;
+    LaneBand b;
+    b.E = E;
+    b.dmin = (delta < 0 ? delta : 0) - h - 1;
+    b.dmax = (delta > 0 ? delta : 0) + h + 1;
+    return b;
+}
+
+__host__ __device__ __forceinline__ int lane_slots(int dmin, int dmax, int nb) {
+    const int p = (dmax - dmin + 127 + 63) / 64;
+    return p < nb ? p : nb;
+}
+
+// Scratch of one lane task: 16-byte {VP, HP} records [column][slot][lane], then one
+// reverse-run list of (m_max + n_max + 2) words per lane.
+__host__ __device__ __forceinline__ uint64_t lane_task_need(int n_max, int m_max, int P) {
+    const uint64_t rec = (static_cast<uint64_t>(n_max) * P * 512 + 255) & ~255ull;
+    const uint64_t runs = (32ull * static_cast<uint64_t>(m_max + n_max + 2) * 4 + 255) & ~255ull;
+    return rec + runs;
+}
+
+// Scratch of one pair in the warp-group Myers kernel with every block stored (redo).
+__host__ __device__ __forceinline__ uint64_t myers_full_need(int m, int n) {
+    const uint64_t nb = static_cast<uint64_t>((m + 63) >> 6);
+    uint64_t need = (static_cast<uint64_t>(n) * nb * 16 + 15) & ~15ull;
+    if (nb > 32) need += (static_cast<uint64_t>(n) + 15) & ~15ull;
+    need += (static_cast<uint64_t>(m + n + 2) * 4 + 15) & ~15ull;
+    return need;
+}
+
 void launch_myers(const ExtendParams& p, int grid, int block, cudaStream_t st);
+void launch_myers_lane(const ExtendParams& p, int grid, cudaStream_t st);
+constexpr int kLaneThreads = 256;
 void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
