@@ -105,7 +105,7 @@ def dp_cells(p):
 
 
 def input_bytes(p):
-    return int(p.seq.nbytes + p.q_off.nbytes + p.q_len.nbytes + p.t_off.nbytes + p.t_len.nbytes)
+    return int(p.seq.nbytes + p.q_off.nbytes + p.q_len.nbytes + p.t_off.nbytes + p.t_len.nbytes + 8 * p.n)
 
 
 def packed_bytes(p):
@@ -295,7 +295,11 @@ def run_engine(args, rank, world):
             t = torch.empty(src.shape, dtype=torch.from_numpy(src[:1]).dtype, pin_memory=True)
             t.numpy()[...] = src
             arrs[k] = t
-        pp = PackedPairs.from_arrays(*(arrs[k].numpy() for k in ("seq", "q_off", "q_len", "t_off", "t_len")))
+        for k in ("q_seed", "t_seed"):  # zero seeds, pinned like the rest (pageable copies would block)
+            arrs[k] = torch.zeros(p.n, dtype=torch.int32, pin_memory=True)
+        pp = PackedPairs.from_arrays(*(arrs[k].numpy() for k in ("seq", "q_off", "q_len", "t_off", "t_len")),
+                                     q_seed=arrs["q_seed"].numpy().view(np.uint32),
+                                     t_seed=arrs["t_seed"].numpy().view(np.uint32))
         pp._pins = arrs
         return pp
 

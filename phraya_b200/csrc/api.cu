@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "engine.cuh"
@@ -13,16 +14,10 @@ namespace {
 
 phr_status check_ctx(phr_ctx* c) { return c ? PHR_OK : PHR_ERR_ARG; }
 
-// Copies a host pair batch into the context's io arena and returns device views.
-phr_status upload_pairs(Ctx* ctx, const phr_pair_batch* b, phr::DevPairs* dp, uint64_t* sum_qt, size_t extra) {
+// Copies a host pair batch (bounds already checked) into the context's io arena and
+// returns device views.
+phr_status upload_pairs(Ctx* ctx, const phr_pair_batch* b, phr::DevPairs* dp, size_t extra) {
     const uint64_t n = b->n_pairs;
-    uint64_t s = 0;
-    for (uint64_t i = 0; i < n; ++i) s += static_cast<uint64_t>(b->q_len[i]) + b->t_len[i];
-    *sum_qt = s;
-    for (uint64_t i = 0; i < n; ++i) {
-        if (b->q_off[i] + b->q_len[i] > b->seq_bytes || b->t_off[i] + b->t_len[i] > b->seq_bytes)
-            return phr::set_error(ctx, PHR_ERR_ARG, "pair " + std::to_string(i) + " reaches past seq_bytes");
-    }
     const size_t need = b->seq_bytes + 64 + n * (8 + 4 + 8 + 4 + 4 + 4) + 8 * 256 + extra;
     ctx->io.reset();
     PHR_CUDA_TRY(ctx, ctx->io.reserve(need));
@@ -59,23 +54,81 @@ bool valid_engine(phr_engine e) {
            e == PHR_ENGINE_MYERS_GLOBAL;
 }
 
-phr_status extend_host(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
-                       phr_result_arena* out) {
+// One chunk of a pipelined host batch: pairs [a, b), sequence bytes [lo, hi).
+struct HostChunk {
+    uint64_t a, b, lo, hi, sum_qt;
+};
+
+// One pass over a host batch on up to 16 threads: bounds of every pair, and per segment
+// of consecutive pairs its byte span and length sum. Returns the first pair that reaches
+// past seq_bytes (n when none).
+struct HostSeg {
+    uint64_t a, b, lo, hi, sum_qt, bad;
+};
+
+uint64_t scan_host_batch(const phr_pair_batch* b, std::vector<HostSeg>* segs, uint64_t nseg) {
+    const uint64_t n = b->n_pairs;
+    nseg = std::max<uint64_t>(1, std::min(nseg, n));
+    segs->assign(nseg, HostSeg{0, 0, UINT64_MAX, 0, 0, n});
+    auto work = [&](uint64_t s0, uint64_t s1) {
+        for (uint64_t s = s0; s < s1; ++s) {
+            HostSeg& g = (*segs)[s];
+            g.a = n * s / nseg;
+            g.b = n * (s + 1) / nseg;
+            for (uint64_t i = g.a; i < g.b; ++i) {
+                const uint64_t qe = b->q_off[i] + b->q_len[i], te = b->t_off[i] + b->t_len[i];
+                if ((qe > b->seq_bytes || te > b->seq_bytes) && g.bad == n) g.bad = i;
+                g.lo = std::min(g.lo, std::min(b->q_off[i], b->t_off[i]));
+                g.hi = std::max(g.hi, std::max(qe, te));
+                g.sum_qt += static_cast<uint64_t>(b->q_len[i]) + b->t_len[i];
+            }
+        }
+    };
+    const uint64_t nthr = std::min<uint64_t>(std::min<uint64_t>(16, std::max(1u, std::thread::hardware_concurrency())),
+                                             n >= (1u << 16) ? nseg : 1);
+    if (nthr <= 1) {
+        work(0, nseg);
+    } else {
+        std::vector<std::thread> th;
+        for (uint64_t t = 0; t < nthr; ++t) th.emplace_back(work, nseg * t / nthr, nseg * (t + 1) / nthr);
+        for (std::thread& x : th) x.join();
+    }
+    uint64_t bad = n;
+    for (const HostSeg& g : *segs) bad = std::min(bad, g.bad);
+    return bad;
+}
+
+// Groups consecutive segments into chunks of about `target` sequence bytes each.
+std::vector<HostChunk> plan_chunks(const std::vector<HostSeg>& segs, uint64_t target) {
+    std::vector<HostChunk> out;
+    HostChunk c{0, 0, UINT64_MAX, 0, 0};
+    for (const HostSeg& g : segs) {
+        if (g.b == g.a) continue;
+        const uint64_t nlo = std::min(c.lo, g.lo), nhi = std::max(c.hi, g.hi);
+        if (c.b > c.a && nhi - nlo > target) {
+            out.push_back(c);
+            c = HostChunk{g.a, g.a, g.lo, g.hi, 0};
+        } else {
+            c.lo = nlo;
+            c.hi = nhi;
+        }
+        c.b = g.b;
+        c.sum_qt += g.sum_qt;
+    }
+    if (c.b > c.a) out.push_back(c);
+    return out;
+}
+
+// Host batch in one piece: copy in, align, copy out.
+phr_status extend_host_whole(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                             phr_result_arena* out, uint64_t sum_qt) {
     Ctx* ctx = &c->impl;
-    if (!batch || !out || (batch->n_pairs && (!batch->q_off || !batch->q_len || !batch->t_off || !batch->t_len ||
-                                               !out->aln || (!batch->seq && batch->seq_bytes))))
-        return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena pointer");
-    if (!valid_engine(engine)) return phr::set_error(ctx, PHR_ERR_ARG, "unknown engine");
-    out->cigar_used = 0;
     const uint64_t n = batch->n_pairs;
-    if (n == 0) return PHR_OK;
-    uint64_t sum_qt = 0;
-    for (uint64_t i = 0; i < n; ++i) sum_qt += static_cast<uint64_t>(batch->q_len[i]) + batch->t_len[i];
     // device output: alignments + worst-case packed text, in the io arena after the inputs
     const uint64_t text_cap = std::min<uint64_t>(out->cigar_capacity, 2 * sum_qt + 16 * n);
     const size_t extra = n * sizeof(phr_alignment) + text_cap + 1024;
     phr::DevPairs dp;
-    phr_status s = upload_pairs(ctx, batch, &dp, &sum_qt, extra);
+    phr_status s = upload_pairs(ctx, batch, &dp, extra);
     if (s != PHR_OK) return s;
     phr::DevResults r;
     r.aln = static_cast<phr_alignment*>(ctx->io.take(n * sizeof(phr_alignment)));
@@ -91,6 +144,165 @@ phr_status extend_host(phr_ctx* c, phr_engine engine, const phr_pair_batch* batc
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     out->cigar_used = r.cigar_used;
     return PHR_OK;
+}
+
+// Host batch in chunks through two device slots: while chunk c aligns on the context
+// stream, chunk c+1's inputs travel host -> device on copy_in and chunk c-1's results
+// device -> host on copy_out. Results are identical to the one-piece path: pairs are
+// independent, and each chunk's CIGAR text lands right after the previous chunk's.
+phr_status extend_host_chunked(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                               phr_result_arena* out, const std::vector<HostChunk>& ch) {
+    Ctx* ctx = &c->impl;
+    for (cudaStream_t* sp : {&ctx->copy_in, &ctx->copy_out})
+        if (!*sp) PHR_CUDA_TRY(ctx, cudaStreamCreateWithFlags(sp, cudaStreamNonBlocking));
+    const bool seeds_q = batch->q_seed != nullptr, seeds_t = batch->t_seed != nullptr;
+    uint64_t max_span = 0, max_n = 0, max_text = 0;
+    for (const HostChunk& k : ch) {
+        max_span = std::max(max_span, k.hi - k.lo);
+        max_n = std::max(max_n, k.b - k.a);
+        max_text = std::max(max_text, std::min<uint64_t>(out->cigar_capacity, 2 * k.sum_qt + 16 * (k.b - k.a)));
+    }
+    auto a256 = [](uint64_t x) { return (x + 511) / 256 * 256; };
+    const uint64_t slot_in = a256(max_span + 64) + 2 * a256(max_n * 8) + 4 * a256(max_n * 4);
+    const uint64_t slot_out = a256(max_n * sizeof(phr_alignment)) + a256(max_text + 16);
+    ctx->io.reset();
+    PHR_CUDA_TRY(ctx, ctx->io.reserve(2 * (slot_in + slot_out) + 4096));
+    struct Slot {
+        uint8_t* seq;
+        uint64_t *qo, *to;
+        uint32_t *ql, *tl, *qs, *ts;
+        phr_alignment* aln;
+        char* cig;
+    } slot[2];
+    for (Slot& sl : slot) {
+        sl.seq = static_cast<uint8_t*>(ctx->io.take(max_span + 64));
+        sl.qo = static_cast<uint64_t*>(ctx->io.take(max_n * 8));
+        sl.to = static_cast<uint64_t*>(ctx->io.take(max_n * 8));
+        sl.ql = static_cast<uint32_t*>(ctx->io.take(max_n * 4));
+        sl.tl = static_cast<uint32_t*>(ctx->io.take(max_n * 4));
+        sl.qs = static_cast<uint32_t*>(ctx->io.take(max_n * 4));
+        sl.ts = static_cast<uint32_t*>(ctx->io.take(max_n * 4));
+        sl.aln = static_cast<phr_alignment*>(ctx->io.take(max_n * sizeof(phr_alignment)));
+        sl.cig = static_cast<char*>(ctx->io.take(max_text + 16));
+        if (!sl.seq || !sl.qo || !sl.to || !sl.ql || !sl.tl || !sl.qs || !sl.ts || !sl.aln || !sl.cig)
+            return phr::set_error(ctx, PHR_ERR_OOM, "io arena exhausted");
+    }
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr}, ev_done = nullptr;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->copy_in);
+        cudaStreamSynchronize(ctx->copy_out);
+        for (cudaEvent_t e : {ev_in[0], ev_in[1], ev_out[0], ev_out[1], ev_done})
+            if (e) cudaEventDestroy(e);
+    };
+    phr_status st = PHR_OK;
+    auto fail = [&](phr_status s) {
+        cleanup();
+        return s;
+    };
+    for (cudaEvent_t* e : {&ev_in[0], &ev_in[1], &ev_out[0], &ev_out[1], &ev_done})
+        if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess)
+            return fail(phr::cuda_status(ctx, cudaGetLastError(), "cudaEventCreate"));
+    auto upload = [&](size_t ci) -> cudaError_t {
+        const HostChunk& k = ch[ci];
+        const Slot& sl = slot[ci & 1];
+        const uint64_t m = k.b - k.a;
+        cudaStream_t s = ctx->copy_in;
+        cudaError_t e = cudaMemcpyAsync(sl.seq, batch->seq + k.lo, k.hi - k.lo, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.qo, batch->q_off + k.a, m * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.ql, batch->q_len + k.a, m * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.to, batch->t_off + k.a, m * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sl.tl, batch->t_len + k.a, m * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && seeds_q) e = cudaMemcpyAsync(sl.qs, batch->q_seed + k.a, m * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && seeds_t) e = cudaMemcpyAsync(sl.ts, batch->t_seed + k.a, m * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_in[ci & 1], s);
+        return e;
+    };
+    {
+        phr::HostScope hs(ctx, "host:e2e_first_uploads");
+        for (size_t ci = 0; ci < std::min<size_t>(2, ch.size()); ++ci)
+            if (cudaError_t e = upload(ci); e != cudaSuccess) return fail(phr::cuda_status(ctx, e, "chunk upload"));
+    }
+    uint64_t base = 0;
+    for (size_t ci = 0; ci < ch.size(); ++ci) {
+        const HostChunk& k = ch[ci];
+        const Slot& sl = slot[ci & 1];
+        const uint64_t m = k.b - k.a;
+        cudaError_t e = cudaStreamWaitEvent(ctx->stream, ev_in[ci & 1], 0);
+        if (e == cudaSuccess && ci >= 2) e = cudaStreamWaitEvent(ctx->stream, ev_out[ci & 1], 0);
+        if (e != cudaSuccess) return fail(phr::cuda_status(ctx, e, "chunk wait"));
+        phr::DevPairs dp;
+        dp.n = m;
+        // offsets stay absolute: the slot holds bytes [lo, hi) at sl.seq
+        dp.seq = reinterpret_cast<const uint8_t*>(reinterpret_cast<uintptr_t>(sl.seq) - k.lo);
+        dp.seq_bytes = k.hi;
+        dp.q_off = sl.qo;
+        dp.q_len = sl.ql;
+        dp.t_off = sl.to;
+        dp.t_len = sl.tl;
+        dp.q_seed = seeds_q ? sl.qs : nullptr;
+        dp.t_seed = seeds_t ? sl.ts : nullptr;
+        phr::DevResults r;
+        r.aln = sl.aln;
+        r.cigar = sl.cig;
+        r.cigar_capacity = std::min<uint64_t>(out->cigar_capacity - base, max_text);
+        r.cigar_base = base;
+        {
+            phr::HostScope hs(ctx, "host:e2e_run_extend");
+            st = phr::run_extend(ctx, engine, dp, costs, &r, k.sum_qt);
+        }
+        if (st != PHR_OK) return fail(st);
+        e = cudaEventRecord(ev_done, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, ev_done, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out->aln + k.a, sl.aln, m * sizeof(phr_alignment), cudaMemcpyDeviceToHost,
+                                ctx->copy_out);
+        if (e == cudaSuccess && r.cigar_used)
+            e = cudaMemcpyAsync(out->cigar + base, sl.cig, r.cigar_used, cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_out[ci & 1], ctx->copy_out);
+        if (e != cudaSuccess) return fail(phr::cuda_status(ctx, e, "chunk download"));
+        base += r.cigar_used;
+        // this slot's inputs were consumed by the (synchronous) alignment above
+        if (ci + 2 < ch.size())
+            if (cudaError_t e2 = upload(ci + 2); e2 != cudaSuccess) return fail(phr::cuda_status(ctx, e2, "chunk upload"));
+    }
+    {
+        phr::HostScope hs(ctx, "host:e2e_drain");
+        cleanup();
+    }
+    if (cudaError_t e = cudaGetLastError(); e != cudaSuccess) return phr::cuda_status(ctx, e, "chunked batch");
+    out->cigar_used = base;
+    return PHR_OK;
+}
+
+phr_status extend_host(phr_ctx* c, phr_engine engine, const phr_pair_batch* batch, phr_affine_costs costs,
+                       phr_result_arena* out) {
+    Ctx* ctx = &c->impl;
+    if (!batch || !out || (batch->n_pairs && (!batch->q_off || !batch->q_len || !batch->t_off || !batch->t_len ||
+                                               !out->aln || (!batch->seq && batch->seq_bytes))))
+        return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena pointer");
+    if (!valid_engine(engine)) return phr::set_error(ctx, PHR_ERR_ARG, "unknown engine");
+    out->cigar_used = 0;
+    const uint64_t n = batch->n_pairs;
+    if (n == 0) return PHR_OK;
+    std::vector<HostSeg> segs;
+    {
+        phr::HostScope hs(ctx, "host:e2e_scan");
+        const uint64_t bad = scan_host_batch(batch, &segs, 64);
+        if (bad < n) return phr::set_error(ctx, PHR_ERR_ARG, "pair " + std::to_string(bad) + " reaches past seq_bytes");
+    }
+    // batches of more than kChunkMin sequence bytes run in about four overlapped chunks
+    constexpr uint64_t kChunkMin = 64ull << 20;
+    if (batch->seq_bytes > 2 * kChunkMin) {
+        const std::vector<HostChunk> ch = plan_chunks(segs, std::max<uint64_t>(kChunkMin, batch->seq_bytes / 4));
+        uint64_t span = 0;
+        for (const HostChunk& k : ch) span += k.hi - k.lo;
+        // chunks whose pairs reference scattered bytes would copy more than the batch: one piece
+        if (ch.size() > 1 && span <= batch->seq_bytes + batch->seq_bytes / 4)
+            return extend_host_chunked(c, engine, batch, costs, out, ch);
+    }
+    uint64_t sum_qt = 0;
+    for (const HostSeg& g : segs) sum_qt += g.sum_qt;
+    return extend_host_whole(c, engine, batch, costs, out, sum_qt);
 }
 
 }  // namespace

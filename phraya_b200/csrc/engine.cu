@@ -108,6 +108,8 @@ Ctx::~Ctx() {
     }
     if (d_counters) cudaFree(d_counters);
     if (h_pinned) cudaFreeHost(h_pinned);
+    if (copy_in) cudaStreamDestroy(copy_in);
+    if (copy_out) cudaStreamDestroy(copy_out);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -467,6 +469,7 @@ struct FinishParams {
     char* cigar;
     uint64_t cigar_capacity;
     uint32_t* error_flag;
+    uint64_t cigar_base;
 };
 
 __global__ void text_len_kernel(const PairOut* out, uint64_t n, uint64_t* len) {
@@ -500,7 +503,7 @@ __global__ void finish_kernel(FinishParams F) {
         phr_alignment a;
         a.status = o.status;
         a.edit_distance = o.status == PHR_OK ? static_cast<uint32_t>(o.ed) : 0;
-        a.cigar_off = off;
+        a.cigar_off = F.cigar_base + off;
         a.cigar_len = len;
         a.affine_score = o.status == PHR_OK ? static_cast<uint32_t>(o.affine_score) : 0;
         if (F.engine == PHR_ENGINE_MYERS_GLOBAL) {
@@ -556,6 +559,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     res->cigar_used = 0;
     if (n == 0) return PHR_OK;
     if (n > 0xFFFFFFF0ull) return set_error(ctx, PHR_ERR_ARG, "too many pairs in one batch");
+    HostScope hs_setup(ctx, "host:extend_setup");
     DeviceArena& A = ctx->arena;
     A.reset();
     PHR_CUDA_TRY(ctx, A.reserve(extend_arena_need(n, in.seq_bytes, sum_qt)));
@@ -674,6 +678,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_ranges, cnt, sizeof(h_ranges), cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     PHR_CUDA_TRY(ctx, cudaGetLastError());
+    hs_setup.stop();
     {
         uint64_t n_tasks = 0;  // tasks of the main pass with a scratch need
         for (int b = 0; b < 64; ++b) n_tasks += h_hist[b];
@@ -878,6 +883,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         }
     }
 
+    hs_redo.stop();
+    HostScope hs_tail(ctx, "host:extend_tail");
     // pack CIGAR text
     {
         KernelScope ks(ctx, "text_len");
@@ -894,7 +901,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (h_total > res->cigar_capacity)
         return set_error(ctx, PHR_ERR_CAPACITY, "CIGAR arena too small: need " + std::to_string(h_total) + " bytes");
-    FinishParams F{n, engine, desc, pout, tbo, text, cigoff, res->aln, res->cigar, res->cigar_capacity, cnt + 10};
+    FinishParams F{n,           engine,     desc,       pout,    tbo, text, cigoff, res->aln, res->cigar,
+                   res->cigar_capacity, cnt + 10, res->cigar_base};
     {
         KernelScope ks(ctx, "finish");
         finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);

@@ -47,6 +47,8 @@ struct Ctx {
     int device = 0;
     int sm_count = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_in = nullptr;    // host -> device copies of pipelined host batches
+    cudaStream_t copy_out = nullptr;   // device -> host copies of their results
     DeviceArena arena;       // per-call temporaries
     DeviceArena scratch;     // per-warp slots of the persistent kernels
     DeviceArena io;          // device copies of host inputs / outputs
@@ -103,12 +105,14 @@ struct HostScope {
     HostScope(Ctx* c, const char* n) : ctx(c), name(n), on(c->timing) {
         if (on) t0 = std::chrono::steady_clock::now();
     }
-    ~HostScope() {
+    void stop() {
         if (!on) return;
+        on = false;
         auto& t = ctx->timings[name];
         t.first += 1;
         t.second += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
+    ~HostScope() { stop(); }
 };
 
 // Device-resident description of a pair batch (pointers into device memory).
@@ -131,6 +135,7 @@ struct DevResults {
     char* cigar = nullptr;         // packed text (device)
     uint64_t cigar_capacity = 0;
     uint64_t cigar_used = 0;       // written (host value) by run_extend
+    uint64_t cigar_base = 0;       // added to every cigar_off (text placed after earlier chunks)
 };
 
 // Runs `engine` over the device batch, writing device results. Synchronizes the
