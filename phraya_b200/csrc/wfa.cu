@@ -167,8 +167,8 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
         if (go) {
             const int32_t* pv_frame = hvf(s - 1);
             int32_t* cur_frame = hvf(s);
-            // lane gl handles diagonals k with (k + tn) % G == gl
-            int k = lo + ((gl - ((lo + tn) % G)) % G + G) % G;
+            // lane gl handles diagonals k with (k + tn) mod G == gl (G is a power of two)
+            int k = lo + ((gl - lo - tn) & (G - 1));
             for (; k <= hi; k += G) {
                 int32_t best_pos = UNSET;
                 uint32_t best_op = 0;
@@ -601,15 +601,53 @@ struct AffDir {
     LayerBand L[3];
 };
 
-__device__ __forceinline__ bool aff_valid(int32_t pos, int k, int qn, int tn) {
-    if (pos == UNSET || pos < 0 || pos > qn) return false;
-    const int tp = pos - k;
-    return tp >= 0 && tp <= tn;
+
+// Directory entry of one score with 32-bit cell indices, kept in a per-group shared
+// ring for the recurrence (which looks back at most max(X, O + E) scores).
+struct SBand {
+    int lo, hi;
+    uint32_t base;
+};
+struct SDir {
+    SBand L[3];
+};
+constexpr int kAffRing = 16;          // scores per ring (power of two)
+constexpr int kAffRingGroups = 8;     // rings per warp: groups of 4 or more lanes
+constexpr int kWarpSeqWords = 1024;   // shared sequence words per warp, split among its groups
+
+// 32 bits holding symbols [pos, pos + kPerWord) of a sequence in shared or global memory.
+template <class S>
+__device__ __forceinline__ uint32_t window_any(const uint32_t* base, int32_t pos) {
+    const uint32_t w = static_cast<uint32_t>(pos) / S::kPerWord;
+    const uint32_t sh = (static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits;
+    return __funnelshift_r(base[w], base[w + 1], sh);
+}
+
+// extend closure (wfa_simd.rs:252-262) for a valid position (0 <= qp <= qn, 0 <= qp-k <= tn).
+template <class S>
+__device__ __forceinline__ int32_t extend_valid(const uint32_t* q, int32_t qn, const uint32_t* t, int32_t tn,
+                                                int32_t qp, int32_t k) {
+    const int32_t tp = qp - k;
+    const int32_t lim = min(qn - qp, tn - tp);
+    int32_t n = 0;
+    while (n < lim) {
+        const uint32_t x = window_any<S>(q, qp + n) ^ window_any<S>(t, tp + n);
+        if (x != 0) return qp + min(n + static_cast<int32_t>(__ffs(x) - 1) / S::kBits, lim);
+        n += S::kPerWord;
+    }
+    return qp + lim;
+}
+
+// affine_pos_valid (wfa_simd.rs:563-569); UNSET and UNSET + 1 are negative, so invalid.
+__device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
+    return static_cast<uint32_t>(pos) <= static_cast<uint32_t>(qn) &&
+           static_cast<uint32_t>(pos) - static_cast<uint32_t>(k) <= static_cast<uint32_t>(tn);
 }
 
 template <class S>
 __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint32_t pid, bool act, int G,
-                                 uint8_t* region, uint64_t region_bytes) {
+                                 uint8_t* region, uint64_t region_bytes, SDir* ring, uint32_t* sseq,
+                                 int sseq_words) {
     const int gl = lane_id() & (G - 1);
     const int qn = act ? d.qn : 0, tn = act ? d.tn : 0;
     const bool fitting = act && tn > qn + qn / 2 + 10;
@@ -617,6 +655,23 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
     const uint32_t* qb = seq_base<S>(P, d.q_word);
     const uint32_t* tb = seq_base<S>(P, d.t_word);
     const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
+    // both sequences into the group's shared words when they fit (one extra word each:
+    // windows read one word past the last symbol; the arena pads every sequence)
+    {
+        const int qw = act ? (qn + S::kPerWord - 1) / S::kPerWord + 1 : 0;
+        const int tw = act ? (tn + S::kPerWord - 1) / S::kPerWord + 1 : 0;
+        const bool stage = sseq != nullptr && qw + tw <= sseq_words;
+        if (stage) {
+            for (int i = gl; i < qw; i += G) sseq[i] = qb[i];
+            for (int i = gl; i < tw; i += G) sseq[qw + i] = tb[i];
+        }
+        __syncwarp();
+        if (stage) {
+            qb = sseq;
+            tb = sseq + qw;
+        }
+    }
+    const bool use_ring = ring != nullptr && O + E < kAffRing && X < kAffRing;
 
     // region: [runs][cells int2 = {value, aux} growing up ...  ... directory growing down]
     // Directory entry of score s is dir_top[-1 - s]; cells and directory share the space.
@@ -626,16 +681,22 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
     int2* cells = reinterpret_cast<int2*>(region + runs_bytes);
     AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + (rest / sizeof(AffDir)) * sizeof(AffDir));
     const uint64_t dir_cap = rest / sizeof(AffDir);
-    const uint64_t cell_cap = rest / 8;
+    // cell indices stay 32-bit: a region never holds more than 2^32 - 1 cells here
+    const uint64_t cell_cap = min(rest / 8, static_cast<uint64_t>(0xFFFFFFFFu));
     auto dir_at = [&](int64_t sc) -> AffDir& { return dir_top[-1 - sc]; };
     auto fits = [&](uint64_t ncells, int64_t nscores) -> bool {
-        return ncells * 8 + static_cast<uint64_t>(nscores) * sizeof(AffDir) <= rest;
+        return ncells <= cell_cap && ncells * 8 + static_cast<uint64_t>(nscores) * sizeof(AffDir) <= rest;
+    };
+    auto band_of = [&](int64_t sc, int layer) -> SBand {
+        if (use_ring) return ring[sc & (kAffRing - 1)].L[layer];
+        const LayerBand& b = dir_at(sc).L[layer];
+        return SBand{b.lo, b.hi, static_cast<uint32_t>(b.base)};
     };
 
     bool alive = act;
     bool done = false, overflow = false;
     int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
-    uint64_t used = 0;
+    uint32_t used = 0;
 
     if (alive && (dir_cap < 1 || cell_cap < 1 || !fits(1, 1))) {
         overflow = true;
@@ -654,7 +715,8 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         e.L[2].hi = 0;
         e.L[2].base = 1;
         dir_at(0) = e;
-        cells[0] = make_int2(wfa_extend<S>(qb, qn, tb, tn, 0, 0), 0);
+        if (use_ring) ring[0] = SDir{{{0, 0, 0u}, {1, 0, 1u}, {1, 0, 1u}}};
+        cells[0] = make_int2(extend_valid<S>(qb, qn, tb, tn, 0, 0), 0);
     }
     __syncwarp();
     if (alive) {
@@ -675,27 +737,36 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
             layer_end = 0;
         }
     }
-    int64_t s = 1;
+    const SBand none = {1, 0, 0u};
+    // every reachable score is a sum of X, O + E and E: a multiple of g = gcd(X, O, E).
+    // Other scores have empty wavefronts (and are never looked up nor traced back), so
+    // the loop visits multiples of g only.
+    int g = 0;
+    for (int v : {X, O, E}) {
+        int a = g, b = v < 0 ? -v : v;
+        while (b) {
+            const int t = a % b;
+            a = b;
+            b = t;
+        }
+        g = a;
+    }
+    const int step = g > 0 ? g : 1;
+    int64_t s = step;
     for (;;) {
         const bool run = alive && !done && s <= hard_max_s;
         if (!__any_sync(PHR_FULL_MASK, run)) break;
-        LayerBand bI = {1, 0, 0}, bD = {1, 0, 0}, bM = {1, 0, 0};
-        LayerBand sMo = {1, 0, 0}, sIe = {1, 0, 0}, sDe = {1, 0, 0}, sMx = {1, 0, 0};
-        if (run) {
-            if (!fits(used, s + 1)) {
-                overflow = true;
-                alive = false;
-            }
-        }
-        bool go = run && alive;
+        SBand bI = none, bD = none, bM = none;
+        SBand sMo = none, sIe = none, sDe = none, sMx = none;
+        bool go = run;
         if (go) {
             const int64_t so = s - O - E, se = s - E, sx = s - X;
-            if (so >= 0) sMo = dir_at(so).L[0];
+            if (so >= 0) sMo = band_of(so, 0);
             if (se >= 0) {
-                sIe = dir_at(se).L[1];
-                sDe = dir_at(se).L[2];
+                sIe = band_of(se, 1);
+                sDe = band_of(se, 2);
             }
-            if (sx >= 0) sMx = dir_at(sx).L[0];
+            if (sx >= 0) sMx = band_of(sx, 0);
             // I: from M[so] (k-1) and I[se] (k-1): bands shifted by +1
             int lo = INT32_MAX, hi = INT32_MIN;
             if (sMo.lo <= sMo.hi) { lo = min(lo, sMo.lo + 1); hi = max(hi, sMo.hi + 1); }
@@ -717,13 +788,13 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
             if (bD.lo <= bD.hi) { lo = min(lo, bD.lo); hi = max(hi, bD.hi); }
             bM.lo = max(lo, -tn);
             bM.hi = min(hi, qn);
-            const uint64_t wI = bI.lo <= bI.hi ? static_cast<uint64_t>(bI.hi - bI.lo + 1) : 0;
-            const uint64_t wD = bD.lo <= bD.hi ? static_cast<uint64_t>(bD.hi - bD.lo + 1) : 0;
-            const uint64_t wM = bM.lo <= bM.hi ? static_cast<uint64_t>(bM.hi - bM.lo + 1) : 0;
+            const uint32_t wI = bI.lo <= bI.hi ? static_cast<uint32_t>(bI.hi - bI.lo + 1) : 0;
+            const uint32_t wD = bD.lo <= bD.hi ? static_cast<uint32_t>(bD.hi - bD.lo + 1) : 0;
+            const uint32_t wM = bM.lo <= bM.hi ? static_cast<uint32_t>(bM.hi - bM.lo + 1) : 0;
             bI.base = used;
             bD.base = used + wI;
             bM.base = used + wI + wD;
-            if (!fits(used + wI + wD + wM, s + 1)) {
+            if (!fits(static_cast<uint64_t>(used) + wI + wD + wM, s + 1)) {
                 overflow = true;
                 alive = false;
                 go = false;
@@ -733,48 +804,33 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         }
         int best_end_k = INT32_MAX, best_end_layer = 0;
         if (go && bM.lo <= bM.hi) {
-            // union band == M band (it contains the I and D bands)
+            // union band == M band (it contains the I and D bands); lane gl takes the
+            // diagonals k with (k + tn) mod G == gl (G is a power of two)
             const int lo = bM.lo, hi = bM.hi;
-            int k = lo + ((gl - ((lo + tn) % G)) % G + G) % G;
-            for (; k <= hi; k += G) {
+            for (int k = lo + ((gl - lo - tn) & (G - 1)); k <= hi; k += G) {
                 int32_t ins = UNSET, del = UNSET;
-                int32_t iop = 0, dop = 0;
                 if (k >= bI.lo && k <= bI.hi) {
-                    int32_t best = UNSET;
-                    if (k - 1 >= -tn) {
-                        if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
-                            const int32_t pv = cells[sMo.base + (k - 1 - sMo.lo)].x;
-                            if (pv != UNSET) {
-                                const int32_t c = pv + 1;
-                                if (aff_valid(c, k, qn, tn) && c > best) { best = c; iop = 0; }
-                            }
-                        }
-                        if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
-                            const int32_t pv = cells[sIe.base + (k - 1 - sIe.lo)].x;
-                            if (pv != UNSET) {
-                                const int32_t c = pv + 1;
-                                if (aff_valid(c, k, qn, tn) && c > best) { best = c; iop = 1; }
-                            }
-                        }
+                    int32_t best = UNSET, iop = 0;
+                    if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
+                        const int32_t c = cells[sMo.base + (k - 1 - sMo.lo)].x + 1;
+                        if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 0; }
+                    }
+                    if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
+                        const int32_t c = cells[sIe.base + (k - 1 - sIe.lo)].x + 1;
+                        if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 1; }
                     }
                     ins = best;
                     cells[bI.base + (k - bI.lo)] = make_int2(ins, iop);
                 }
                 if (k >= bD.lo && k <= bD.hi) {
-                    int32_t best = UNSET;
-                    if (k + 1 <= qn) {
-                        if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
-                            const int32_t pv = cells[sMo.base + (k + 1 - sMo.lo)].x;
-                            if (pv != UNSET) {
-                                if (aff_valid(pv, k, qn, tn) && pv > best) { best = pv; dop = 0; }
-                            }
-                        }
-                        if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
-                            const int32_t pv = cells[sDe.base + (k + 1 - sDe.lo)].x;
-                            if (pv != UNSET) {
-                                if (aff_valid(pv, k, qn, tn) && pv > best) { best = pv; dop = 1; }
-                            }
-                        }
+                    int32_t best = UNSET, dop = 0;
+                    if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
+                        const int32_t c = cells[sMo.base + (k + 1 - sMo.lo)].x;
+                        if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 0; }
+                    }
+                    if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
+                        const int32_t c = cells[sDe.base + (k + 1 - sDe.lo)].x;
+                        if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 1; }
                     }
                     del = best;
                     cells[bD.base + (k - bD.lo)] = make_int2(del, dop);
@@ -783,30 +839,24 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
                 int32_t best = UNSET;
                 uint32_t mop = 0;
                 if (k >= sMx.lo && k <= sMx.hi) {
-                    const int32_t pv = cells[sMx.base + (k - sMx.lo)].x;
-                    if (pv != UNSET) {
-                        const int32_t c = pv + 1;
-                        if (aff_valid(c, k, qn, tn) && c > best) { best = c; mop = 0; }
-                    }
+                    const int32_t c = cells[sMx.base + (k - sMx.lo)].x + 1;
+                    if (pos_ok(c, k, qn, tn)) { best = c; mop = 0; }
                 }
-                if (ins != UNSET && aff_valid(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
-                if (del != UNSET && aff_valid(del, k, qn, tn) && del > best) { best = del; mop = 2; }
+                if (pos_ok(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
+                if (pos_ok(del, k, qn, tn) && del > best) { best = del; mop = 2; }
                 int32_t mval = UNSET;
                 uint32_t aux = 0;
                 if (best != UNSET) {
-                    mval = wfa_extend<S>(qb, qn, tb, tn, best, k);
+                    mval = extend_valid<S>(qb, qn, tb, tn, best, k);
                     aux = (static_cast<uint32_t>(best) << 2) | mop;
                 }
                 cells[bM.base + (k - bM.lo)] = make_int2(mval, static_cast<int32_t>(aux));
                 // endpoint candidates: value == qn in layer order m, ins, del
-                int layer = -1;
-                if (mval == qn) layer = 0;
-                else if (ins == qn) layer = 1;
-                else if (del == qn) layer = 2;
+                const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
                 if (layer >= 0) {
                     if (!fitting) {
                         if (k == qn - tn) { best_end_k = k; best_end_layer = layer; }
-                    } else if (k >= qn - tn && k <= qn && k < best_end_k) {
+                    } else if (k >= qn - tn && k < best_end_k) {
                         best_end_k = k;
                         best_end_layer = layer;
                     }
@@ -815,10 +865,11 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         }
         if (go && gl == 0) {
             AffDir e;
-            e.L[0] = bM;
-            e.L[1] = bI;
-            e.L[2] = bD;
+            e.L[0] = LayerBand{bM.lo, bM.hi, bM.base};
+            e.L[1] = LayerBand{bI.lo, bI.hi, bI.base};
+            e.L[2] = LayerBand{bD.lo, bD.hi, bD.base};
             dir_at(s) = e;
+            if (use_ring) ring[s & (kAffRing - 1)] = SDir{{bM, bI, bD}};
         }
         // group min over (k, layer): smallest k wins (largest t_end)
         int kk = best_end_k, ll = best_end_layer;
@@ -835,14 +886,14 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
             k_end = kk;
             layer_end = ll;
         }
-        if (run) ++s;
+        if (run) s += step;
     }
     const bool failed = act && !done && !overflow;
     if (act && overflow && gl == 0) {
         // retry with 4x the room used so far (bounded by every diagonal of every score)
         const uint64_t full = runs_bytes + static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
                               static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull;
-        const uint64_t grow = runs_bytes + 4ull * (used * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) + 4096;
+        const uint64_t grow = runs_bytes + 4ull * (static_cast<uint64_t>(used) * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) + 4096;
         report_redo(P, pid, min(full, grow));
     }
 
@@ -941,8 +992,11 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
 }
 
 // Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
+constexpr int kAffWarpSmem = kAffRingGroups * kAffRing * static_cast<int>(sizeof(SDir)) + kWarpSeqWords * 4;
+
 template <class S, bool kAffine>
 __global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams P) {
+    extern __shared__ __align__(16) uint8_t wfa_smem[];
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     for (;;) {
@@ -978,8 +1032,15 @@ __global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams 
             if (act && (lane & (G - 1)) == 0) report_redo(P, pid, P.task_need[task] / (32 / G));
             continue;
         }
-        if (kAffine)
-            wfa_affine_group<S>(P, d, pid, act, G, region, region_bytes);
+        if (kAffine) {
+            // per warp: one directory ring per group of >= 4 lanes, then the sequence words
+            uint8_t* wsm = wfa_smem + static_cast<size_t>(threadIdx.x >> 5) * kAffWarpSmem;
+            SDir* ring = G >= 4 ? reinterpret_cast<SDir*>(wsm) + grp * kAffRing : nullptr;
+            const int seq_words = kWarpSeqWords / (32 / G);
+            uint32_t* sseq = reinterpret_cast<uint32_t*>(wsm + kAffRingGroups * kAffRing * sizeof(SDir)) +
+                             grp * seq_words;
+            wfa_affine_group<S>(P, d, pid, act, G, region, region_bytes, ring, sseq, seq_words);
+        }
         else
             wfa_linear_group<S>(P, d, pid, act, G, region, region_bytes);
     }
@@ -1005,10 +1066,14 @@ void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream
     }
 }
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st) {
-    wfa_kernel<Seq2, true><<<grid, block, 0, st>>>(p);
+    const int smem = (block / 32) * kAffWarpSmem;
+    cudaFuncSetAttribute(wfa_kernel<Seq2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    wfa_kernel<Seq2, true><<<grid, block, smem, st>>>(p);
 }
 void launch_wfa_affine_bytes(const ExtendParams& p, int grid, int block, cudaStream_t st) {
-    wfa_kernel<SeqB, true><<<grid, block, 0, st>>>(p);
+    const int smem = (block / 32) * kAffWarpSmem;
+    cudaFuncSetAttribute(wfa_kernel<SeqB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    wfa_kernel<SeqB, true><<<grid, block, smem, st>>>(p);
 }
 
 }  // namespace phr
