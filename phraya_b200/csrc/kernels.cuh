@@ -86,6 +86,10 @@ __host__ __device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool
 // P = ceil((dmax - dmin + 127) / 64) query blocks of 64 rows per column (at most nb).
 // ---------------------------------------------------------------------------
 constexpr int kLaneMaxSlots = 8;
+// Records of kLaneColGroup consecutive columns of one lane and slot are adjacent. One
+// column per group measured fastest on B200: grouping two or four columns halves the
+// traceback's sector reads but the forward pass's interleaved stores cost more.
+constexpr int kLaneColGroup = 1;
 
 struct LaneBand {
     int E;
@@ -110,10 +114,11 @@ __host__ __device__ __forceinline__ int lane_slots(int dmin, int dmax, int nb) {
     return p < nb ? p : nb;
 }
 
-// Scratch of one lane task: 16-byte {VP, HP} records [column][slot][lane], then one
-// reverse-run list of (m_max + n_max + 2) words per lane.
+// Scratch of one lane task: 16-byte {VP, HP} records [column group][slot][lane][column
+// in group], then one reverse-run list of (m_max + n_max + 2) words per lane.
 __host__ __device__ __forceinline__ uint64_t lane_task_need(int n_max, int m_max, int P) {
-    const uint64_t rec = (static_cast<uint64_t>(n_max) * P * 512 + 255) & ~255ull;
+    const uint64_t ng = static_cast<uint64_t>((n_max + kLaneColGroup - 1) / kLaneColGroup);
+    const uint64_t rec = (ng * kLaneColGroup * P * 512 + 255) & ~255ull;
     const uint64_t runs = (32ull * static_cast<uint64_t>(m_max + n_max + 2) * 4 + 255) & ~255ull;
     return rec + runs;
 }

@@ -32,9 +32,10 @@
 // D'(m, n) >= ed > E. Either way the pair is redone by the warp-group kernel with
 // every block (myers.cu), so every reported result equals the reference's.
 //
-// Records. Per column and slot a 16-byte {VP, HP} record ([column][slot][lane],
-// coalesced 512-byte stores); VP bit r is D[r+1][j] - D[r][j] == +1 ("cur == above
-// + 1"), HP bit r is D[r+1][j] - D[r+1][j-1] == +1 ("cur == left + 1").
+// Records. Per column and slot a 16-byte {VP, HP} record, laid out [column group][slot]
+// [lane][column in group] (kLaneColGroup columns per group; with one, a warp's stores of
+// one column and slot are 512 contiguous bytes). VP bit r is D[r+1][j] - D[r][j] == +1
+// ("cur == above + 1"), HP bit r is D[r+1][j] - D[r+1][j-1] == +1 ("cur == left + 1").
 #include "kernels.cuh"
 
 namespace phr {
@@ -108,6 +109,13 @@ __device__ __forceinline__ uint64_t advance_block(uint64_t& vp, uint64_t& vn, ui
     return ph;
 }
 
+// Byte offset of the record of column index j0 (column j0 + 1), slot k, lane `lane`.
+template <int P>
+__device__ __forceinline__ uint64_t rec_off(int j0, int k, int lane) {
+    return (static_cast<uint64_t>(j0 / kLaneColGroup) * P + k) * (512 * kLaneColGroup) + lane * (16 * kLaneColGroup) +
+           (j0 % kLaneColGroup) * 16;
+}
+
 struct LaneGeom {
     int P;        // blocks in the window
     int dmin, dmax;
@@ -146,7 +154,7 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
     if (g.slide && P < nb) load_block_words(qb, P, qn);
     uint32_t tw = 0;
     uint32_t tw_next = n > 0 ? __ldg(tb) : 0u;
-    uint8_t* r = rec + lane * 16;
+    uint8_t* r = rec + lane * (16 * kLaneColGroup);   // current column group of this lane
     for (int j = 1; j <= g.n_max; ++j) {
         if (j == next_shift) {  // warp-uniform: drop the top block, a new block enters
 #pragma unroll
@@ -175,15 +183,17 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
         }
         const uint32_t c = (tw >> ((jj & 15) * 2)) & 3u;
         const uint64_t* eqp = sp + c * 32 + lane;
+        const int sub = jj % kLaneColGroup;
         uint32_t pa = 0, ma = 0;
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const uint64_t eq = eqp[k * 128];
             const uint64_t ph = k == 0 ? advance_block<true>(vp[0], vn[0], eq, pa, ma)
                                        : advance_block<false>(vp[k], vn[k], eq, pa, ma);
-            *reinterpret_cast<uint4*>(r + k * 512) = make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(ph), hi32(ph));
+            *reinterpret_cast<uint4*>(r + k * (512 * kLaneColGroup) + sub * 16) =
+                make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(ph), hi32(ph));
         }
-        r += P * 512;
+        if (sub == kLaneColGroup - 1) r += P * (512 * kLaneColGroup);
     }
 }
 
@@ -222,7 +232,7 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
                 if (jt > 0) {
                     const int k = b - lane_blo(g, jt);
                     if (k >= 0 && k < P) {
-                        const uint8_t* src = rec + (static_cast<uint64_t>(jt - 1) * P + k) * 512 + lane * 16;
+                        const uint8_t* src = rec + rec_off<P>(jt - 1, k, lane);
                         const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(srec + t * 32));
                         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
                         valid |= 1u << t;
@@ -320,7 +330,8 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     const uint32_t* tb = Pm.packed2 + (act ? d.t_word : 0);
     lane_forward<P>(qb, tb, n, nb, g, sp, slot);
     __syncwarp();  // the traceback reuses the Peq shared memory
-    const uint64_t rec_bytes = (static_cast<uint64_t>(g.n_max) * P * 512 + 255) & ~255ull;
+    const uint64_t ng = static_cast<uint64_t>((g.n_max + kLaneColGroup - 1) / kLaneColGroup);
+    const uint64_t rec_bytes = (ng * kLaneColGroup * P * 512 + 255) & ~255ull;
     const uint32_t cap = static_cast<uint32_t>(g.m_max + g.n_max + 2);
     uint32_t* runs = reinterpret_cast<uint32_t*>(slot + rec_bytes) + static_cast<uint64_t>(lane) * cap;
     RunWriter rw;
