@@ -126,6 +126,15 @@ def roofline(name, step_ms, launches, work, set_a, set_b, int_peak, hbm_peak, pe
         t_int, t_hbm = ops / int_peak, nbytes / hbm_peak
         work_txt = ("band cells = 64 x block-columns evaluated (kernel counter); int ops = cells x 22/32; "
                     "bytes = 16 B {VP,HP} record per block-column + 16 B read back per target column + 2-bit inputs")
+    elif name in ("wfa_affine", "wfa_linear"):
+        cells, words = work[name + "_cells"], work[name + "_lcp_words"]
+        per = 30.0 if name == "wfa_affine" else 10.0   # ops per wavefront diagonal (3 layers / 1)
+        ops = per * cells + 4.0 * words                # + 4 ops per word compare of match extension
+        nbytes = packed_bytes(set_a) + 40.0 * set_a.n  # 2-bit inputs + one alignment record per pair
+        t_int, t_hbm = ops / int_peak, nbytes / hbm_peak
+        work_txt = (f"wavefront diagonals x {per:.0f} ops + LCP word compares x 4 ops (kernel counters); "
+                    "bytes = 2-bit inputs + result records")
+        cols = None
     else:
         return {"kernel": name, "kernel_ms_per_step": step_ms, "bound": None,
                 "note": "no work counter for this kernel"}
@@ -143,11 +152,15 @@ def roofline(name, step_ms, launches, work, set_a, set_b, int_peak, hbm_peak, pe
         # distribution (6.34 GB), scaled by the pair count
         traffic = 6.34e9 * set_b.n / 100000
         traffic_src = "ncu capture of 100,000 pairs (6.34 GB), scaled by pairs"
-    return {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
-            "traffic": traffic, "traffic_source": traffic_src, "kernel": name, "kernel_ms_per_step": step_ms,
-            "launches_per_step": launches, "work": work_txt, "peak_source": psrc,
-            "int_frac": ops / sec / int_peak, "hbm_frac": nbytes / sec / hbm_peak,
-            "band_cells_per_step": cols * 64, "redo_pairs_per_step": work["myers_lane_redo_pairs"]}
+    out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
+           "traffic": traffic, "traffic_source": traffic_src, "kernel": name, "kernel_ms_per_step": step_ms,
+           "launches_per_step": launches, "work": work_txt, "peak_source": psrc,
+           "int_frac": ops / sec / int_peak, "hbm_frac": nbytes / sec / hbm_peak}
+    if name == "myers_lane":
+        out.update(band_cells_per_step=cols * 64, redo_pairs_per_step=work["myers_lane_redo_pairs"])
+    else:
+        out.update(wavefront_diagonals_per_step=work[name + "_cells"], lcp_words_per_step=work[name + "_lcp_words"])
+    return out
 
 
 def cpu_baseline(set_a, set_b, n_a, n_b, nthreads, sample_a=60000, sample_b=6000):
@@ -284,7 +297,9 @@ def run_engine(args, rank, world):
     ktimes = {recs[i].name.decode(): (recs[i].launches, recs[i].total_ms) for i in range(min(nrec, 64))
               if not recs[i].name.startswith(b"host:")}
     # work counters of the timed steps (reset with the timings)
-    work = {k: eng.counter(k) / args.steps for k in ("myers_lane_block_columns", "myers_lane_redo_pairs")}
+    work = {k: eng.counter(k) / args.steps for k in ("myers_lane_block_columns", "myers_lane_redo_pairs",
+                                                      "wfa_affine_cells", "wfa_affine_lcp_words",
+                                                      "wfa_linear_cells", "wfa_linear_lcp_words")}
 
     # ---- end to end through the host API, pinned host buffers ----------------
     def pinned_pairs(p):
@@ -351,6 +366,9 @@ def run_engine(args, rank, world):
     hbm_peak = peaks.get("hbm_gbs", 6650.0) * 1e9                      # bytes/s, measured copy
     roof = roofline(name, step_ms, ktimes[name][0] / args.steps, work, set_a, set_b, int_peak, hbm_peak,
                     peak_src, args.traffic_gb_per_step)
+    # the other extension kernels, each against its own bound
+    roofs = {k: roofline(k, kms[k], ktimes[k][0] / args.steps, work, set_a, set_b, int_peak, hbm_peak, peak_src)
+             for k in ("myers_lane", "wfa_affine", "wfa_linear") if k in kms}
     pipe = None
     if not args.no_pipeline:
         pipe = run_pipeline(eng, dev, args)
@@ -367,6 +385,7 @@ def run_engine(args, rank, world):
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1000.0},
             "gpu_launches": launches,
             "roofline": roof,
+            "rooflines": roofs,
             "kernel_ms": {k: round(v[1] / args.steps, 3) for k, v in ktimes.items()},
             "clocks": clk,
             "cpu_baseline": cpu,

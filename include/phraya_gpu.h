@@ -125,6 +125,9 @@ void phr_ctx_destroy(phr_ctx* ctx);
  * kernels are CPU code with nothing to tune); results never depend on them. Keys:
  *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen
  *                                        wfa_long_min (power of two, 1..32)
+ *   "wfa_affine_group_short"             lanes per gap-affine WFA pair below that edge
+ *                                        (power of two, 1..32; "wfa_group_short" is then
+ *                                        the linear engine's)
  *   "wfa_long_min"                       that length-bucket edge (default 1024)
  *   "myers_band_base"                    Myers stored-band half-width base (>= 0)
  *   "block_threads"                      threads per block of the warp-per-pair kernels
@@ -163,7 +166,9 @@ void phr_ctx_reset_timing(phr_ctx* ctx);
  * Work counters accumulated over the context's extension calls (no counterpart in the
  * reference): "myers_lane_block_columns" counts the 64-row block x column steps the
  * banded Myers kernel evaluated (64 DP cells each); "myers_lane_redo_pairs" the pairs
- * it handed to the every-block redo pass. Unknown names read 0.
+ * it handed to the every-block redo pass; "wfa_affine_cells" / "wfa_linear_cells" count
+ * wavefront diagonals computed (the M band of each score) and "wfa_affine_lcp_words" /
+ * "wfa_linear_lcp_words" the word compares of match extension. Unknown names read 0.
  */
 uint64_t phr_ctx_counter(const phr_ctx* ctx, const char* name);
 /* The cudaStream_t the context launches on (for callers that order their own work). */

@@ -371,6 +371,7 @@ phr_status phr_ctx_create(int32_t device, const phr_config* cfg, phr_ctx** out) 
 namespace {
 int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "wfa_group_short")) return &t.wfa_group_short;
+    if (!std::strcmp(key, "wfa_affine_group_short")) return &t.wfa_affine_group_short;
     if (!std::strcmp(key, "wfa_group_long")) return &t.wfa_group_long;
     if (!std::strcmp(key, "myers_band_base")) return &t.myers_band_base;
     if (!std::strcmp(key, "block_threads")) return &t.block_threads;
@@ -381,7 +382,8 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
-    if (!std::strcmp(key, "wfa_group_short") || !std::strcmp(key, "wfa_group_long"))
+    if (!std::strcmp(key, "wfa_group_short") || !std::strcmp(key, "wfa_group_long") ||
+        !std::strcmp(key, "wfa_affine_group_short"))
         return v >= 1 && v <= 32 && (v & (v - 1)) == 0;
     if (!std::strcmp(key, "myers_band_base")) return v >= 0 && v <= (1 << 20);
     if (!std::strcmp(key, "block_threads")) return v >= 32 && v <= 256 && v % 32 == 0;

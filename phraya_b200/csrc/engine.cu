@@ -629,7 +629,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     // counters: [0..3] ranges, [4] split_min, [5] queue head 0, [6] queue head 1,
     // [7] redo count, [8..9] need max (u64), [10] error flag, [12..13] total (u64), [14..17] redo ranges,
     // [20] first multi-lane 2-bit task, [24..25] CTA-kernel queue heads, [26] lane-kernel queue head,
-    // [28..31] lane-kernel and warp-group 2-bit ranges (global Myers), [32..35] work counters (u64)
+    // [28..31] lane-kernel and warp-group 2-bit ranges (global Myers), [32..39] work counters (u64)
     uint32_t* cnt = static_cast<uint32_t*>(take(256));
     if (!cnt) return set_error(ctx, PHR_ERR_OOM, "device arena exhausted");
     unsigned long long* need_max = reinterpret_cast<unsigned long long*>(cnt + 8);
@@ -650,6 +650,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     if (!tmp) return set_error(ctx, PHR_ERR_OOM, "device arena exhausted (cub)");
 
     const unsigned T = 256;
+    // lanes per short WFA pair: affine and linear tune separately
+    const int g_short = engine == PHR_ENGINE_WFA_AFFINE ? ctx->tune.wfa_affine_group_short : ctx->tune.wfa_group_short;
     PrepParams pp{in, engine, costs, desc, pout, w2, wb, tb};
     {
         KernelScope ks(ctx, "prep_sizes");
@@ -663,7 +665,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     cub::DeviceScan::ExclusiveSum(tmp, tn_, tb, tbo, static_cast<int>(n), st);
 
     PackParams pk{in, engine, costs, desc, pout, w2o, wbo, tbo, arena2, arenab, text, keys, vals,
-                  ctx->tune.wfa_group_short, ctx->tune.wfa_group_long, ctx->tune.wfa_long_min,
+                  g_short, ctx->tune.wfa_group_long, ctx->tune.wfa_long_min,
                   ctx->tune.myers_band_base};
     {
         KernelScope ks(ctx, "pack");
@@ -894,7 +896,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             {
                 KernelScope ks(ctx, "redo_tasks");
                 redo_tasks_kernel<<<blocks_for(m, T), T, 0, st>>>(rlist2, cnt + 18, desc, engine,
-                                                                 ctx->tune.wfa_group_short, ctx->tune.wfa_group_long,
+                                                                 g_short, ctx->tune.wfa_group_long,
                                                                  ctx->tune.wfa_long_min,
                                                                  P.big_min, P.big_smem, task_first, task_count,
                                                                  task_group, cnt + 14);
@@ -939,12 +941,17 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
     }
     uint32_t h_err = 0;
-    unsigned long long h_work[2] = {0, 0};
+    unsigned long long h_work[4] = {0, 0, 0, 0};
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_err, cnt + 10, 4, cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(h_work, cnt + 32, sizeof(h_work), cudaMemcpyDeviceToHost, st));
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (h_work[0]) ctx->counters["myers_lane_block_columns"] += h_work[0];
     if (h_work[1]) ctx->counters["myers_lane_redo_pairs"] += h_work[1];
+    if (h_work[2] || h_work[3]) {
+        const std::string e = engine == PHR_ENGINE_WFA_AFFINE ? "wfa_affine" : "wfa_linear";
+        ctx->counters[e + "_cells"] += h_work[2];
+        ctx->counters[e + "_lcp_words"] += h_work[3];
+    }
     PHR_CUDA_TRY(ctx, cudaGetLastError());
     if (ctx->timing) ctx->resolve_timings();
     if (h_err) return set_error(ctx, PHR_ERR_CUDA, "internal consistency check failed (flags " + std::to_string(h_err) + ")");

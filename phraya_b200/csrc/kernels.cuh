@@ -41,7 +41,8 @@ struct ExtendParams {
     uint32_t* error_flag;       // set on an internal inconsistency (bounded loops ran out)
     int32_t big_min;            // linear WFA: pairs with qn+tn >= big_min run one per CTA (0: off)
     uint32_t big_smem;          // dynamic shared memory of the CTA-per-pair kernel (bytes)
-    unsigned long long* work;   // [0] banded Myers block-columns, [1] pairs sent to redo
+    unsigned long long* work;   // [0] banded Myers block-columns, [1] pairs sent to redo,
+                                // [2] WFA wavefront diagonals, [3] WFA LCP word compares
 };
 
 // task_group bit marking a redo task for the CTA-per-pair kernel

@@ -73,6 +73,31 @@ __device__ __forceinline__ void report_redo(const ExtendParams& P, uint32_t pid,
     if (P.redo_need) P.redo_need[k] = need;
 }
 
+// 32 bits holding symbols [pos, pos + kPerWord) of a sequence in shared or global memory.
+template <class S>
+__device__ __forceinline__ uint32_t window_any(const uint32_t* base, int32_t pos) {
+    const uint32_t w = static_cast<uint32_t>(pos) / S::kPerWord;
+    const uint32_t sh = (static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits;
+    return __funnelshift_r(base[w], base[w + 1], sh);
+}
+
+// extend closure (wfa_simd.rs:252-262) for a valid position (0 <= qp <= qn, 0 <= qp-k <= tn).
+// `words` counts the word compares (the LCP work of the roofline).
+template <class S>
+__device__ __forceinline__ int32_t extend_valid(const uint32_t* q, int32_t qn, const uint32_t* t, int32_t tn,
+                                                int32_t qp, int32_t k, uint32_t& words) {
+    const int32_t tp = qp - k;
+    const int32_t lim = min(qn - qp, tn - tp);
+    int32_t n = 0;
+    while (n < lim) {
+        ++words;
+        const uint32_t x = window_any<S>(q, qp + n) ^ window_any<S>(t, tp + n);
+        if (x != 0) return qp + min(n + static_cast<int32_t>(__ffs(x) - 1) / S::kBits, lim);
+        n += S::kPerWord;
+    }
+    return qp + lim;
+}
+
 // ===========================================================================
 // Linear WFA
 // ===========================================================================
@@ -109,6 +134,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
 
     // largest score whose frames fit: lin_base(s+1) <= cell_cap
     const int max_s = qn + tn;
+    uint32_t wf_cells = 0, lcp_words = 0;   // work counters: band diagonals, LCP word compares
     bool alive = act;
     bool done = false, overflow = false;
     int s_end = 0, t_end = 0;
@@ -121,7 +147,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
         }
     }
     if (alive && gl == 0) {
-        const int32_t v = wfa_extend<S>(qb, qn, tb, tn, 0, 0);
+        const int32_t v = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
         hvf(0)[0] = v;
         hr[0] = 0;
     }
@@ -164,6 +190,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
         }
         const bool go = run && alive;
         int best_end_k = INT32_MAX;
+        if (go && gl == 0) wf_cells += static_cast<uint32_t>(hi - lo + 1);
         if (go) {
             const int32_t* pv_frame = hvf(s - 1);
             int32_t* cur_frame = hvf(s);
@@ -208,7 +235,7 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
                 if (have) {
                     const int32_t j = best_pos - k;
                     if (!(best_pos < 0 || best_pos > qn || j < 0 || j > tn)) {
-                        val = wfa_extend<S>(qb, qn, tb, tn, best_pos, k);
+                        val = extend_valid<S>(qb, qn, tb, tn, best_pos, k, lcp_words);
                         aux = (static_cast<uint32_t>(best_pos) << 2) | best_op;
                     }
                 }
@@ -233,6 +260,13 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
             t_end = qn - kk;
         }
         if (run) ++s;
+    }
+    {
+        const unsigned cw = __reduce_add_sync(PHR_FULL_MASK, wf_cells), lw = __reduce_add_sync(PHR_FULL_MASK, lcp_words);
+        if (lane_id() == 0 && P.work) {
+            atomicAdd(P.work + 2, static_cast<unsigned long long>(cw));
+            atomicAdd(P.work + 3, static_cast<unsigned long long>(lw));
+        }
     }
     const bool failed = act && !done && !overflow;  // loop exhausted: AlignmentFailed
     if (act && overflow && gl == 0) {
@@ -612,31 +646,11 @@ struct SDir {
     SBand L[3];
 };
 constexpr int kAffRing = 16;          // scores per ring (power of two)
-constexpr int kAffRingGroups = 8;     // rings per warp: groups of 4 or more lanes
-constexpr int kWarpSeqWords = 1024;   // shared sequence words per warp, split among its groups
-
-// 32 bits holding symbols [pos, pos + kPerWord) of a sequence in shared or global memory.
-template <class S>
-__device__ __forceinline__ uint32_t window_any(const uint32_t* base, int32_t pos) {
-    const uint32_t w = static_cast<uint32_t>(pos) / S::kPerWord;
-    const uint32_t sh = (static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits;
-    return __funnelshift_r(base[w], base[w + 1], sh);
-}
-
-// extend closure (wfa_simd.rs:252-262) for a valid position (0 <= qp <= qn, 0 <= qp-k <= tn).
-template <class S>
-__device__ __forceinline__ int32_t extend_valid(const uint32_t* q, int32_t qn, const uint32_t* t, int32_t tn,
-                                                int32_t qp, int32_t k) {
-    const int32_t tp = qp - k;
-    const int32_t lim = min(qn - qp, tn - tp);
-    int32_t n = 0;
-    while (n < lim) {
-        const uint32_t x = window_any<S>(q, qp + n) ^ window_any<S>(t, tp + n);
-        if (x != 0) return qp + min(n + static_cast<int32_t>(__ffs(x) - 1) / S::kBits, lim);
-        n += S::kPerWord;
-    }
-    return qp + lim;
-}
+constexpr int kAffRingGroups = 4;     // rings per warp: groups of 8 or more lanes
+// Shared sequence words per warp, split among its groups. Zero: the sequences are read
+// through L1, which keeps more of the recent wavefront cells when shared memory is small
+// (staging both sequences measured slower: it took L1 capacity from the cells).
+constexpr int kWarpSeqWords = 0;
 
 // affine_pos_valid (wfa_simd.rs:563-569); UNSET and UNSET + 1 are negative, so invalid.
 __device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
@@ -673,19 +687,23 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
     }
     const bool use_ring = ring != nullptr && O + E < kAffRing && X < kAffRing;
 
-    // region: [runs][cells int2 = {value, aux} growing up ...  ... directory growing down]
-    // Directory entry of score s is dir_top[-1 - s]; cells and directory share the space.
+    // region: [runs][values: cap int32][aux: cap uint32][... directory growing down]
+    // The recurrence reads values only; keeping them apart from the traceback's aux words
+    // doubles the cells each cached sector holds. Directory entry of score s is
+    // dir_top[-1 - s], in the last quarter of the region.
     uint32_t* runs = reinterpret_cast<uint32_t*>(region);
     const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
     const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
-    int2* cells = reinterpret_cast<int2*>(region + runs_bytes);
-    AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + (rest / sizeof(AffDir)) * sizeof(AffDir));
-    const uint64_t dir_cap = rest / sizeof(AffDir);
+    const uint64_t dir_cap = (rest / 4) / sizeof(AffDir);
     // cell indices stay 32-bit: a region never holds more than 2^32 - 1 cells here
-    const uint64_t cell_cap = min(rest / 8, static_cast<uint64_t>(0xFFFFFFFFu));
+    const uint64_t cell_bytes = rest - rest % sizeof(AffDir) - dir_cap * sizeof(AffDir);
+    const uint64_t cell_cap = min(static_cast<uint64_t>((cell_bytes / 8) & ~3ull), static_cast<uint64_t>(0xFFFFFFFFu));
+    int32_t* vals = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* auxs = reinterpret_cast<uint32_t*>(vals + cell_cap);
+    AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + rest - (rest % sizeof(AffDir)));
     auto dir_at = [&](int64_t sc) -> AffDir& { return dir_top[-1 - sc]; };
     auto fits = [&](uint64_t ncells, int64_t nscores) -> bool {
-        return ncells <= cell_cap && ncells * 8 + static_cast<uint64_t>(nscores) * sizeof(AffDir) <= rest;
+        return ncells <= cell_cap && static_cast<uint64_t>(nscores) <= dir_cap;
     };
     auto band_of = [&](int64_t sc, int layer) -> SBand {
         if (use_ring) return ring[sc & (kAffRing - 1)].L[layer];
@@ -697,6 +715,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
     bool done = false, overflow = false;
     int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
     uint32_t used = 0;
+    uint32_t wf_cells = 0, lcp_words = 0;   // work counters: M-band diagonals, LCP word compares
 
     if (alive && (dir_cap < 1 || cell_cap < 1 || !fits(1, 1))) {
         overflow = true;
@@ -716,12 +735,13 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         e.L[2].base = 1;
         dir_at(0) = e;
         if (use_ring) ring[0] = SDir{{{0, 0, 0u}, {1, 0, 1u}, {1, 0, 1u}}};
-        cells[0] = make_int2(extend_valid<S>(qb, qn, tb, tn, 0, 0), 0);
+        vals[0] = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
+        auxs[0] = 0;
     }
     __syncwarp();
     if (alive) {
         used = 1;
-        const int v0 = cells[0].x;
+        const int v0 = vals[0];
         // endpoint (wfa_simd.rs:618-650) on frame 0: only diagonal 0 is set
         if (!fitting) {
             if (qn - tn == 0 && v0 == qn) {
@@ -788,6 +808,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
             if (bD.lo <= bD.hi) { lo = min(lo, bD.lo); hi = max(hi, bD.hi); }
             bM.lo = max(lo, -tn);
             bM.hi = min(hi, qn);
+            if (gl == 0 && bM.lo <= bM.hi) wf_cells += static_cast<uint32_t>(bM.hi - bM.lo + 1);
             const uint32_t wI = bI.lo <= bI.hi ? static_cast<uint32_t>(bI.hi - bI.lo + 1) : 0;
             const uint32_t wD = bD.lo <= bD.hi ? static_cast<uint32_t>(bD.hi - bD.lo + 1) : 0;
             const uint32_t wM = bM.lo <= bM.hi ? static_cast<uint32_t>(bM.hi - bM.lo + 1) : 0;
@@ -812,34 +833,36 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
                 if (k >= bI.lo && k <= bI.hi) {
                     int32_t best = UNSET, iop = 0;
                     if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
-                        const int32_t c = cells[sMo.base + (k - 1 - sMo.lo)].x + 1;
+                        const int32_t c = vals[sMo.base + (k - 1 - sMo.lo)] + 1;
                         if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 0; }
                     }
                     if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
-                        const int32_t c = cells[sIe.base + (k - 1 - sIe.lo)].x + 1;
+                        const int32_t c = vals[sIe.base + (k - 1 - sIe.lo)] + 1;
                         if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 1; }
                     }
                     ins = best;
-                    cells[bI.base + (k - bI.lo)] = make_int2(ins, iop);
+                    vals[bI.base + (k - bI.lo)] = ins;
+                    auxs[bI.base + (k - bI.lo)] = static_cast<uint32_t>(iop);
                 }
                 if (k >= bD.lo && k <= bD.hi) {
                     int32_t best = UNSET, dop = 0;
                     if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
-                        const int32_t c = cells[sMo.base + (k + 1 - sMo.lo)].x;
+                        const int32_t c = vals[sMo.base + (k + 1 - sMo.lo)];
                         if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 0; }
                     }
                     if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
-                        const int32_t c = cells[sDe.base + (k + 1 - sDe.lo)].x;
+                        const int32_t c = vals[sDe.base + (k + 1 - sDe.lo)];
                         if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 1; }
                     }
                     del = best;
-                    cells[bD.base + (k - bD.lo)] = make_int2(del, dop);
+                    vals[bD.base + (k - bD.lo)] = del;
+                    auxs[bD.base + (k - bD.lo)] = static_cast<uint32_t>(dop);
                 }
                 // M (wfa_simd.rs:743-765): [mismatch-extend, ins close, del close], strict >
                 int32_t best = UNSET;
                 uint32_t mop = 0;
                 if (k >= sMx.lo && k <= sMx.hi) {
-                    const int32_t c = cells[sMx.base + (k - sMx.lo)].x + 1;
+                    const int32_t c = vals[sMx.base + (k - sMx.lo)] + 1;
                     if (pos_ok(c, k, qn, tn)) { best = c; mop = 0; }
                 }
                 if (pos_ok(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
@@ -847,10 +870,11 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
                 int32_t mval = UNSET;
                 uint32_t aux = 0;
                 if (best != UNSET) {
-                    mval = extend_valid<S>(qb, qn, tb, tn, best, k);
+                    mval = extend_valid<S>(qb, qn, tb, tn, best, k, lcp_words);
                     aux = (static_cast<uint32_t>(best) << 2) | mop;
                 }
-                cells[bM.base + (k - bM.lo)] = make_int2(mval, static_cast<int32_t>(aux));
+                vals[bM.base + (k - bM.lo)] = mval;
+                auxs[bM.base + (k - bM.lo)] = aux;
                 // endpoint candidates: value == qn in layer order m, ins, del
                 const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
                 if (layer >= 0) {
@@ -888,12 +912,21 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         }
         if (run) s += step;
     }
+    {
+        const unsigned cw = __reduce_add_sync(PHR_FULL_MASK, wf_cells), lw = __reduce_add_sync(PHR_FULL_MASK, lcp_words);
+        if (lane_id() == 0 && P.work) {
+            atomicAdd(P.work + 2, static_cast<unsigned long long>(cw));
+            atomicAdd(P.work + 3, static_cast<unsigned long long>(lw));
+        }
+    }
     const bool failed = act && !done && !overflow;
     if (act && overflow && gl == 0) {
         // retry with 4x the room used so far (bounded by every diagonal of every score)
-        const uint64_t full = runs_bytes + static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
-                              static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull;
-        const uint64_t grow = runs_bytes + 4ull * (static_cast<uint64_t>(used) * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) + 4096;
+        const uint64_t full = runs_bytes + 4ull * static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
+                              static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull + 4096;
+        // the directory gets a quarter of the region, the cells the rest
+        const uint64_t grow = runs_bytes + 4ull * (static_cast<uint64_t>(used) * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) +
+                              4096;
         report_redo(P, pid, min(full, grow));
     }
 
@@ -915,8 +948,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
             }
             const AffDir e = dir_at(ss);
             if (layer == 0) {
-                const int2 c = cells[e.L[0].base + (k - e.L[0].lo)];
-                const uint32_t aux = static_cast<uint32_t>(c.y);
+                const uint32_t aux = auxs[e.L[0].base + (k - e.L[0].lo)];
                 const uint32_t mop = aux & 3;
                 const int32_t raw = static_cast<int32_t>(aux >> 2);
                 const int mc = max(qi - raw, 0);
@@ -938,8 +970,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
                 rw.push(3, 1);  // ins (query-extra) -> 'D'
                 --qi;
                 ++n_edit;
-                const int2 c = cells[e.L[1].base + (k - e.L[1].lo)];
-                if (c.y == 0) {
+                if (auxs[e.L[1].base + (k - e.L[1].lo)] == 0) {
                     ss -= O + E;
                     layer = 0;
                 } else {
@@ -950,8 +981,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
                 rw.push(2, 1);  // del (target-extra) -> 'I'
                 --ti;
                 ++n_edit;
-                const int2 c = cells[e.L[2].base + (k - e.L[2].lo)];
-                if (c.y == 0) {
+                if (auxs[e.L[2].base + (k - e.L[2].lo)] == 0) {
                     ss -= O + E;
                     layer = 0;
                 } else {
@@ -1035,10 +1065,11 @@ __global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams 
         if (kAffine) {
             // per warp: one directory ring per group of >= 4 lanes, then the sequence words
             uint8_t* wsm = wfa_smem + static_cast<size_t>(threadIdx.x >> 5) * kAffWarpSmem;
-            SDir* ring = G >= 4 ? reinterpret_cast<SDir*>(wsm) + grp * kAffRing : nullptr;
+            SDir* ring = 32 / G <= kAffRingGroups ? reinterpret_cast<SDir*>(wsm) + grp * kAffRing : nullptr;
             const int seq_words = kWarpSeqWords / (32 / G);
-            uint32_t* sseq = reinterpret_cast<uint32_t*>(wsm + kAffRingGroups * kAffRing * sizeof(SDir)) +
-                             grp * seq_words;
+            uint32_t* sseq = seq_words > 0 ? reinterpret_cast<uint32_t*>(wsm + kAffRingGroups * kAffRing * sizeof(SDir)) +
+                                                 grp * seq_words
+                                           : nullptr;
             wfa_affine_group<S>(P, d, pid, act, G, region, region_bytes, ring, sseq, seq_words);
         }
         else

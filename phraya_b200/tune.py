@@ -24,6 +24,7 @@ from . import api as P
 
 SPACE = {
     "wfa_group_short": [4, 8, 16, 32],
+    "wfa_affine_group_short": [8, 16, 32],
     "wfa_group_long": [16, 32],
     "wfa_long_min": [512, 1024, 2048],
     "block_threads": [128, 256],
@@ -35,7 +36,7 @@ SPACE = {
 KEYS_FOR = {
     A.ENGINE_WFA_LINEAR: ["wfa_group_short", "wfa_group_long", "wfa_long_min", "block_threads",
                           "max_blocks_per_sm", "wfa_big_min"],
-    A.ENGINE_WFA_AFFINE: ["wfa_group_short", "wfa_group_long", "wfa_long_min", "block_threads",
+    A.ENGINE_WFA_AFFINE: ["wfa_affine_group_short", "wfa_group_long", "wfa_long_min", "block_threads",
                           "max_blocks_per_sm"],
     A.ENGINE_MYERS_FIT: ["myers_band_base", "block_threads", "max_blocks_per_sm"],
     A.ENGINE_MYERS_GLOBAL: ["myers_band_base", "block_threads", "max_blocks_per_sm"],

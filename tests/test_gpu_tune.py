@@ -17,6 +17,7 @@ def test_group_sizes_bit_exact(g_short):
     pk = D.extension_pairs(600, 40, 400, 0.08, seed=31)
     with P.Engine(0) as eng:
         eng.set_tune("wfa_group_short", g_short)
+        eng.set_tune("wfa_affine_group_short", g_short)
         eng.set_tune("wfa_long_min", 512)
         eng.set_tune("block_threads", 128)
         for engine, costs in ((A.ENGINE_WFA_LINEAR, (2, 4, 1)), (A.ENGINE_WFA_AFFINE, (4, 6, 2))):
