@@ -42,8 +42,8 @@ namespace phr {
 namespace {
 
 constexpr int kLaneWarps = kLaneThreads / 32;
-constexpr int kTraceCols = 16;  // columns whose records one traceback refill loads
-static_assert(kTraceCols * 32 * 16 <= kLaneMaxSlots * 4 * 32 * 8, "traceback slots exceed the Peq area");
+constexpr int kTraceBatch = 8;  // diagonal cells whose records one traceback fetch loads
+static_assert(2 * kTraceBatch * 32 * 16 <= kLaneMaxSlots * 4 * 32 * 8, "traceback slots exceed the Peq area");
 
 __device__ __forceinline__ uint32_t even_bits(uint32_t x) {
     x &= 0x55555555u;
@@ -197,62 +197,95 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
     }
 }
 
-// Traceback of one lane's pair from (m, n). The walk moves column by column: a column's
-// record holds the VP / HP bits of 64 rows, so D runs stay in one record and I or
-// diagonal moves step to the next column. Records of kTraceCols columns (current
-// block) are fetched together into the lane's shared-memory slots, so one memory
-// latency covers up to kTraceCols columns. Returns false when the walk left the band
-// or cost more than E (the pair is then redone).
+// Issues asynchronous global -> shared copies of the records of the kTraceBatch cells
+// (ci - t, cj - t), t < kTraceBatch, of one diagonal, each from its own block, into
+// buf[t * 32] (one cp.async group). Returns the mask of cells whose record lies in the
+// window (others are left unloaded).
+template <int P>
+__device__ __forceinline__ uint32_t fetch_diagonal(const uint8_t* rec, const LaneGeom& g, int ci, int cj, uint4* buf) {
+    const int lane = lane_id();
+    uint32_t valid = 0;
+#pragma unroll
+    for (int t = 0; t < kTraceBatch; ++t) {
+        const int it = ci - t, jt = cj - t;
+        if (it > 0 && jt > 0) {
+            const int k = ((it - 1) >> 6) - lane_blo(g, jt);
+            if (k >= 0 && k < P) {
+                const uint8_t* src = rec + rec_off<P>(jt - 1, k, lane);
+                const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(buf + t * 32));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+                valid |= 1u << t;
+            }
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    return valid;
+}
+
+// 2-bit symbols [pos - 8, pos + 8) of a sequence shifted so that symbol pos - 1 - t sits
+// at index 7 - t (t < 8) also when pos < 8 (lower indices then hold zeros).
+__device__ __forceinline__ uint32_t diag_window(const uint32_t* __restrict__ s, int pos) {
+    const int p0 = pos > 8 ? pos - 8 : 0;
+    return load_window<Seq2>(s, p0) << (2 * (8 - (pos - p0)));
+}
+
+// Traceback of one lane's pair from (m, n). The records the walk needs lie along
+// diagonals between indels, so they are fetched kTraceBatch cells of the current
+// diagonal at a time, each cell's record from its own block, and the next batch of the
+// same diagonal is prefetched while this one is processed (two shared-memory buffers
+// per lane). A D run is read off one record; an I move, or a D run, starts a new
+// diagonal. Returns false when the walk left the band or cost more than E (the pair is
+// then redone).
 template <int P>
 __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, const uint32_t* __restrict__ tb, int m,
                                            int n, const LaneBand& band, const LaneGeom& g, bool act,
                                            const uint8_t* rec, uint4* srec, RunWriter& rw, int* ed_out) {
-    const int lane = lane_id();
     int i = act ? m : 0, j = act ? n : 0, cost = 0;
     bool ok = act;
-    int j0 = -1, bwin = -1;          // window: columns (j0 - kTraceCols, j0] of block bwin
-    uint32_t valid = 0;              // bit t: record of column j0 - t is inside the window
-    uint32_t twin = 0;               // target symbols [tbase, tbase + 16)
-    int tbase = 0;
-    uint64_t qwin = 0;               // query symbols [qbase, qbase + 32)
-    int qbase = 0x7fffffff;
+    uint4* bufA = srec;                      // batch starting at cell (ai, aj)
+    uint4* bufB = srec + kTraceBatch * 32;   // the next batch of the same diagonal
+    int ai = -1, aj = -1;
+    uint32_t va = 0, vb = 0;                 // loaded-cell masks
+    uint32_t xa = 0, xb = 0;                 // query XOR target symbols: cell t at index 7 - t
     for (;;) {
         const bool want = ok && i > 0 && j > 0;
         if (!__any_sync(PHR_FULL_MASK, want)) break;
         if (!want) continue;
-        const int b = (i - 1) >> 6;
-        if (j0 < 0 || j <= j0 - kTraceCols || b != bwin) {
-            j0 = j;
-            bwin = b;
-            valid = 0;
-            // asynchronous global -> shared copies: all columns in flight at once, no registers
-#pragma unroll
-            for (int t = 0; t < kTraceCols; ++t) {
-                const int jt = j - t;
-                if (jt > 0) {
-                    const int k = b - lane_blo(g, jt);
-                    if (k >= 0 && k < P) {
-                        const uint8_t* src = rec + rec_off<P>(jt - 1, k, lane);
-                        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(srec + t * 32));
-                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-                        valid |= 1u << t;
-                    }
-                }
+        int t = ai - i;
+        if (!(ai >= 0 && ai - i == aj - j && t >= 0 && t < kTraceBatch)) {
+            if (ai >= 0 && ai - i == aj - j && t >= kTraceBatch && t < 2 * kTraceBatch) {
+                // the walk went on along the diagonal into the prefetched batch
+                uint4* x = bufA;
+                bufA = bufB;
+                bufB = x;
+                ai -= kTraceBatch;
+                aj -= kTraceBatch;
+                va = vb;
+                xa = xb;
+                asm volatile("cp.async.wait_all;\n" ::: "memory");
+            } else {
+                // a new diagonal: this batch and the next
+                ai = i;
+                aj = j;
+                va = fetch_diagonal<P>(rec, g, ai, aj, bufA);
+                xa = diag_window(qb, ai) ^ diag_window(tb, aj);
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
             }
-            asm volatile("cp.async.wait_all;\n" ::: "memory");
-            tbase = j > 16 ? j - 16 : 0;
-            twin = load_window<Seq2>(tb, tbase);
+            vb = fetch_diagonal<P>(rec, g, ai - kTraceBatch, aj - kTraceBatch, bufB);
+            xb = (ai - kTraceBatch > 0 && aj - kTraceBatch > 0)
+                     ? diag_window(qb, ai - kTraceBatch) ^ diag_window(tb, aj - kTraceBatch)
+                     : 0u;
+            t = ai - i;
         }
-        const int t = j0 - j;
-        if (!((valid >> t) & 1u)) {
+        if (!((va >> t) & 1u)) {
             ok = false;
             continue;
         }
-        const uint4 R = srec[t * 32];
+        const uint4 R = bufA[t * 32];
         const uint64_t vp = mk64(R.x, R.y), hp = mk64(R.z, R.w);
         const int bit = (i - 1) & 63;
         if ((vp >> bit) & 1ull) {
-            // D run: consecutive VP bits upward from row i within this block
+            // D run: consecutive VP bits upward from row i within this record's block
             const int run = __clzll(~(vp << (63 - bit)));
             rw.push(3, static_cast<uint32_t>(run));
             i -= run;
@@ -262,32 +295,24 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
             j -= 1;
             cost += 1;
         } else {
-            // diagonal stretch: cells (i-u, j-u) of this window and block, u < L
-            const int L = min(min(kTraceCols - t, bit + 1), min(i, j));
+            // diagonal stretch over the cells t + u of this batch: stop at the first cell
+            // with a VP or HP bit, without a record, or past the batch
+            const int L = min(kTraceBatch - t, min(i, j));
             uint32_t stop = 0;
 #pragma unroll
-            for (int u = 1; u < kTraceCols; ++u) {
+            for (int u = 1; u < kTraceBatch; ++u) {
                 if (u < L) {
-                    const uint4 Q = srec[(t + u) * 32];
+                    const uint4 Q = bufA[(t + u) * 32];
                     const uint64_t sv = mk64(Q.x | Q.z, Q.y | Q.w);
-                    stop |= static_cast<uint32_t>((sv >> (bit - u)) & 1ull) << u;
+                    stop |= static_cast<uint32_t>((sv >> ((i - 1 - u) & 63)) & 1ull) << u;
                 }
             }
-            stop |= ~(valid >> t);            // a cell without a record ends the stretch
-            stop |= ~0u << L;                 // L < 32
-            const int run = __ffs(stop) - 1;  // diagonal moves (>= 1: cell u = 0 is one)
-            // M / X per cell: query symbols i-16 .. i-1 against target symbols j-16 .. j-1
-            if ((i > 16 ? i - 16 : 0) < qbase || i - 1 >= qbase + 32) {
-                qbase = i > 32 ? i - 32 : 0;
-                qwin = mk64(load_window<Seq2>(qb, qbase), load_window<Seq2>(qb, qbase + 16));
-            }
-            const int sq = 2 * (i - 16 - qbase), st = 2 * (j - 16 - tbase);
-            const uint32_t qa = static_cast<uint32_t>(sq >= 0 ? (qwin >> sq) : (qwin << -sq));
-            const uint32_t ta = st >= 0 ? (twin >> st) : (twin << -st);
-            const uint32_t x = qa ^ ta;
-            // symbol k of the aligned words is cell u = 15 - k; bit 2k of nz -> bit 2u+1 reversed
-            const uint32_t nz = (x | (x >> 1)) & 0x55555555u;
-            const uint32_t neq = even_bits(__brev(nz) >> 1);
+            stop |= ~(va >> t);
+            stop |= ~0u << L;
+            const int run = __ffs(stop) - 1;  // >= 1: cell u = 0 is diagonal
+            // M / X: cell t + u compares symbol index 7 - (t + u) of the batch's windows
+            const uint32_t nz = (xa | (xa >> 1)) & 0x55555555u;
+            const uint32_t neq = even_bits(__brev(nz) >> 17) >> t;   // bit u: cell t + u differs
             int u = 0;
             while (u < run) {
                 const uint32_t cur = (neq >> u) & 1u;
@@ -304,6 +329,7 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
         const int d = j - i;
         if (d < band.dmin || d > band.dmax || cost > band.E) ok = false;
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     if (ok) {
         if (i > 0) {
             rw.push(3, static_cast<uint32_t>(i));
@@ -320,6 +346,10 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
     return ok;
 }
 
+// Forward pass and traceback of one task in one warp; records in the warp's slot. (A
+// separate traceback kernel with more resident warps measured slower on B200: the 32
+// lanes' walks diverge, so a traceback warp executes about as many instructions as the
+// forward pass whatever hides its latency.)
 template <int P>
 __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& d, bool act, const LaneBand& band,
                           const LaneGeom& g, uint64_t* sp, uint8_t* slot) {
@@ -329,6 +359,9 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     const uint32_t* qb = Pm.packed2 + (act ? d.q_word : 0);
     const uint32_t* tb = Pm.packed2 + (act ? d.t_word : 0);
     lane_forward<P>(qb, tb, n, nb, g, sp, slot);
+    // work counter: block-columns this task evaluated for its pairs
+    const unsigned long long cols = __reduce_add_sync(PHR_FULL_MASK, act ? static_cast<unsigned>(n) * P : 0u);
+    if (lane == 0) atomicAdd(Pm.work, cols);
     __syncwarp();  // the traceback reuses the Peq shared memory
     const uint64_t ng = static_cast<uint64_t>((g.n_max + kLaneColGroup - 1) / kLaneColGroup);
     const uint64_t rec_bytes = (ng * kLaneColGroup * P * 512 + 255) & ~255ull;
@@ -338,13 +371,9 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     rw.init(runs, static_cast<uint32_t>(m + n + 2), true);
     int ed = 0;
     const bool ok = lane_trace<P>(qb, tb, m, n, band, g, act, slot, reinterpret_cast<uint4*>(sp) + lane, rw, &ed);
-    // work counters: block-columns this task evaluated for its pairs, pairs sent to redo
-    const unsigned long long cols = __reduce_add_sync(PHR_FULL_MASK, act ? static_cast<unsigned>(n) * P : 0u);
+    // work counter: pairs sent to redo
     const unsigned redo = __popc(__ballot_sync(PHR_FULL_MASK, act && !ok));
-    if (lane == 0) {
-        atomicAdd(Pm.work, cols);
-        if (redo) atomicAdd(Pm.work + 1, static_cast<unsigned long long>(redo));
-    }
+    if (lane == 0 && redo) atomicAdd(Pm.work + 1, static_cast<unsigned long long>(redo));
     if (act && !ok) {
         const uint32_t k = atomicAdd(Pm.redo_count, 1u);
         Pm.redo_list[k] = pid;
@@ -377,18 +406,15 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     }
 }
 
-__global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParams Pm) {
-    extern __shared__ uint64_t lane_smem[];
+__device__ __forceinline__ void lane_tasks(const ExtendParams& Pm, uint64_t* sp) {
     const int lane = lane_id();
-    const int wib = threadIdx.x >> 5;
-    uint64_t* sp = lane_smem + static_cast<uint64_t>(wib) * kLaneMaxSlots * 4 * 32;
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    uint8_t* slot = Pm.scratch + warp_global * Pm.slot_bytes;
     for (;;) {
         uint32_t task = 0;
         if (lane == 0) task = Pm.tasks.range[0] + atomicAdd(Pm.queue_head, 1u);
         task = __shfl_sync(PHR_FULL_MASK, task, 0);
         if (task >= Pm.tasks.range[1]) break;
+        uint8_t* slot = Pm.scratch + warp_global * Pm.slot_bytes;
         const int count = Pm.tasks.task_count[task];
         const bool act = lane < count;
         const uint32_t pid = act ? Pm.tasks.order[Pm.tasks.task_first[task] + lane] : 0;
@@ -405,6 +431,7 @@ __global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParam
         g.P = lane_slots(g.dmin, g.dmax, g.nb_max);
         g.slide = g.P < g.nb_max;
         const uint64_t need = lane_task_need(g.n_max, g.m_max, g.P);
+        // a task beyond the kernel's window or its warp slot is redone by the every-block kernel
         if (g.P > kLaneMaxSlots || need > Pm.slot_bytes) {
             if (lane == 0) atomicAdd(Pm.work + 1, static_cast<unsigned long long>(count));
             if (act) {
@@ -430,15 +457,18 @@ __global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParam
     }
 }
 
+constexpr int kLanePeqWarpBytes = kLaneMaxSlots * 4 * 32 * 8;  // Peq (and traceback buffers) per warp
+
+__global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParams Pm) {
+    extern __shared__ uint64_t lane_smem[];
+    lane_tasks(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kLanePeqWarpBytes / 8));
+}
+
 }  // namespace
 
 void launch_myers_lane(const ExtendParams& p, int grid, cudaStream_t st) {
-    const size_t smem = static_cast<size_t>(kLaneWarps) * kLaneMaxSlots * 4 * 32 * sizeof(uint64_t);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(myers_lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        configured = true;
-    }
+    const int smem = kLaneWarps * kLanePeqWarpBytes;
+    cudaFuncSetAttribute(myers_lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     myers_lane_kernel<<<grid, kLaneThreads, smem, st>>>(p);
 }
 
