@@ -149,9 +149,10 @@ def roofline(name, step_ms, launches, work, set_a, set_b, int_peak, hbm_peak, pe
         traffic, traffic_src = traffic_gb * 1e9, "--traffic-gb-per-step"
     elif name == "myers_lane":
         # ncu dram__bytes_read.sum + write.sum of one launch on 100,000 pairs of the same
-        # distribution (6.34 GB), scaled by the pair count
-        traffic = 6.34e9 * set_b.n / 100000
-        traffic_src = "ncu capture of 100,000 pairs (6.34 GB), scaled by pairs"
+        # distribution (3.01 + 4.58 GB, profiles/myers_lane_kernel_set_b_100k.md), scaled by
+        # the pair count
+        traffic = 7.59e9 * set_b.n / 100000
+        traffic_src = "ncu capture of 100,000 pairs (7.59 GB), scaled by pairs"
     out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
            "traffic": traffic, "traffic_source": traffic_src, "kernel": name, "kernel_ms_per_step": step_ms,
            "launches_per_step": launches, "work": work_txt, "peak_source": psrc,
