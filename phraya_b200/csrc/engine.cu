@@ -282,32 +282,33 @@ __global__ void pack_kernel(PackParams P) {
     // from a separate arena take the byte loop)
     const uintptr_t ok_lo = reinterpret_cast<uintptr_t>(P.in.seq);
     const uintptr_t ok_hi = ok_lo + P.in.seq_bytes;
-    for (int side = 0; side < 2; ++side) {
+    // query words then target words, dealt to the warp's lanes as one list
+    const int nwq = (d.qn + 15) / 16, nwt = (d.tn + 15) / 16;
+    for (int x = lane; x < nwq + nwt; x += 32) {
+        const int side = x >= nwq;
+        const int w = side ? x - nwq : x;
         const uint8_t* src = side ? tsrc : qsrc;
         const bool wide = !(side && P.in.t_seq);
         const int len = side ? d.tn : d.qn;
         uint32_t* dst = P.arena2 + w2 + (side ? q2w : 0);
-        const int nw = (len + 15) / 16;
-        for (int w = lane; w < nw; w += 32) {
-            uint32_t word = 0;
-            const int p0 = w * 16;
-            const int lim = min(16, len - p0);
-            const uint8_t* cp = src + p0;
-            const uintptr_t a0 = reinterpret_cast<uintptr_t>(cp) & ~static_cast<uintptr_t>(3);
-            if (wide && lim == 16 && a0 >= ok_lo && a0 + 20 <= ok_hi) {
-                // 16 bases from five aligned words, four bases per step
-                const uint32_t* wp = reinterpret_cast<const uint32_t*>(a0);
-                const uint32_t sh = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(cp) & 3) * 8;
-                uint32_t v[5];
+        uint32_t word = 0;
+        const int p0 = w * 16;
+        const int lim = min(16, len - p0);
+        const uint8_t* cp = src + p0;
+        const uintptr_t a0 = reinterpret_cast<uintptr_t>(cp) & ~static_cast<uintptr_t>(3);
+        if (wide && lim == 16 && a0 >= ok_lo && a0 + 20 <= ok_hi) {
+            // 16 bases from five aligned words, four bases per step
+            const uint32_t* wp = reinterpret_cast<const uint32_t*>(a0);
+            const uint32_t sh = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(cp) & 3) * 8;
+            uint32_t v[5];
 #pragma unroll
-                for (int j = 0; j < 5; ++j) v[j] = __ldg(wp + j);
+            for (int j = 0; j < 5; ++j) v[j] = __ldg(wp + j);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) word |= code2x4(__funnelshift_r(v[j], v[j + 1], sh), pure) << (8 * j);
-            } else {
-                for (int b = 0; b < lim; ++b) word |= code2(cp[b], pure) << (2 * b);
-            }
-            dst[w] = word;
+            for (int j = 0; j < 4; ++j) word |= code2x4(__funnelshift_r(v[j], v[j + 1], sh), pure) << (8 * j);
+        } else {
+            for (int b = 0; b < lim; ++b) word |= code2(cp[b], pure) << (2 * b);
         }
+        dst[w] = word;
     }
     pure = __all_sync(PHR_FULL_MASK, pure);
     if (pure) {

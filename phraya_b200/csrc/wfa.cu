@@ -658,6 +658,112 @@ __device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
            static_cast<uint32_t>(pos) - static_cast<uint32_t>(k) <= static_cast<uint32_t>(tn);
 }
 
+// Traceback (wfa_simd.rs:785-886) of a finished affine wavefront and the pair's result:
+// history in `auxs` through the score directory below `dir_top`. Called by all lanes of
+// the warp; the leader of each group of G lanes walks its pair.
+// With row_g > 0 the history is the register kernel's: the aux word of (score, layer, k)
+// is auxs[(score / row_g) * 3 * row_w + layer * row_w + k - row_lo], no directory read.
+__device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int G, int qn, int tn, int X, int O,
+                              int E, uint32_t* runs, const uint32_t* auxs, const AffDir* dir_top, bool done,
+                              bool failed, int s_end, int t_end, int k_end, int layer_end, int row_g = 0,
+                              int row_w = 0, int row_lo = 0) {
+    const int gl = lane_id() & (G - 1);
+    auto dir_at = [&](int64_t sc) -> const AffDir& { return dir_top[-1 - sc]; };
+    auto aux_at = [&](int ss, int layer, int k) -> uint32_t {
+        if (row_g > 0)
+            return auxs[static_cast<uint64_t>(ss / row_g) * (3 * row_w) + layer * row_w + (k - row_lo)];
+        const LayerBand& b = dir_at(ss).L[layer];
+        return auxs[b.base + (k - b.lo)];
+    };
+    RunWriter rw;
+    rw.init(runs, static_cast<uint32_t>(qn + tn + 2));
+    const bool trace = act && done;
+    uint32_t n_edit = 0;
+    if (trace && gl == 0) {
+        int qi = qn, ti = t_end, k = k_end, ss = s_end, layer = layer_end;
+        int guard = 4 * (qn + tn) + 16;
+        while ((qi > 0 || ti > 0) && guard-- > 0) {
+            if (ss == 0) {
+                const int mm = min(qi, ti);
+                rw.push(0, static_cast<uint32_t>(mm));
+                qi -= mm;
+                ti -= mm;
+                break;
+            }
+            if (layer == 0) {
+                const uint32_t aux = aux_at(ss, 0, k);
+                const uint32_t mop = aux & 3;
+                const int32_t raw = static_cast<int32_t>(aux >> 2);
+                const int mc = max(qi - raw, 0);
+                if (mc > 0) {
+                    rw.push(0, static_cast<uint32_t>(mc));
+                    qi -= mc;
+                    ti -= mc;
+                }
+                if (mop == 0) {
+                    rw.push(1, 1);
+                    --qi;
+                    --ti;
+                    ++n_edit;
+                    ss -= X;
+                } else {
+                    layer = static_cast<int>(mop);
+                }
+            } else if (layer == 1) {
+                rw.push(3, 1);  // ins (query-extra) -> 'D'
+                --qi;
+                ++n_edit;
+                if (aux_at(ss, 1, k) == 0) {
+                    ss -= O + E;
+                    layer = 0;
+                } else {
+                    ss -= E;
+                }
+                k -= 1;
+            } else {
+                rw.push(2, 1);  // del (target-extra) -> 'I'
+                --ti;
+                ++n_edit;
+                if (aux_at(ss, 2, k) == 0) {
+                    ss -= O + E;
+                    layer = 0;
+                } else {
+                    ss -= E;
+                }
+                k += 1;
+            }
+        }
+        if (guard < 0) atomicOr(P.error_flag, 4u);
+        rw.flush();
+    }
+    const int leader = lane_id() & ~(G - 1);
+    const uint32_t nr = __shfl_sync(PHR_FULL_MASK, rw.n, leader);
+    const bool ovf = __shfl_sync(PHR_FULL_MASK, rw.overflow ? 1 : 0, leader) != 0;
+    const uint32_t ned = __shfl_sync(PHR_FULL_MASK, n_edit, leader);
+    __syncwarp();
+    const uint32_t nr_fmt = (trace && !ovf) ? nr : 0;
+    char* out = act ? P.text + P.text_off[pid] : nullptr;
+    const uint32_t tl = format_group(runs, nr_fmt, out, G);
+    if (act && gl == 0) {
+        if (trace && !ovf) {
+            PairOut o;
+            o.status = PHR_OK;
+            o.ed = static_cast<int32_t>(ned);  // levenshtein_from_cigar: X + I/D lengths
+            o.t_consumed = t_end;
+            o.affine_score = s_end;
+            o.n_runs = nr;
+            o.text_len = tl;
+            P.out[pid] = o;
+        } else if (failed) {
+            PairOut o = {};
+            o.status = PHR_ALIGNMENT_FAILED;
+            P.out[pid] = o;
+        } else if (trace && ovf) {
+            atomicOr(P.error_flag, 2u);
+        }
+    }
+}
+
 template <class S>
 __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint32_t pid, bool act, int G,
                                  uint8_t* region, uint64_t region_bytes, SDir* ring, uint32_t* sseq,
@@ -930,102 +1036,231 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
         report_redo(P, pid, min(full, grow));
     }
 
-    // ---- traceback (wfa_simd.rs:785-886) ----
-    RunWriter rw;
-    rw.init(runs, static_cast<uint32_t>(qn + tn + 2));
-    const bool trace = act && done;
-    uint32_t n_edit = 0;
-    if (trace && gl == 0) {
-        int qi = qn, ti = t_end, k = k_end, ss = s_end, layer = layer_end;
-        int guard = 4 * (qn + tn) + 16;
-        while ((qi > 0 || ti > 0) && guard-- > 0) {
-            if (ss == 0) {
-                const int mm = min(qi, ti);
-                rw.push(0, static_cast<uint32_t>(mm));
-                qi -= mm;
-                ti -= mm;
-                break;
+    affine_finish(P, pid, act, G, qn, tn, X, O, E, runs, auxs, dir_top, done, failed, s_end, t_end, k_end,
+                  layer_end);
+}
+
+// ===========================================================================
+// Gap-affine WFA, one pair per warp, wavefronts in registers
+// ===========================================================================
+// Every reachable cell of score s lies on a diagonal |k| <= (s - O) / E (a gap of length
+// L costs O + L E), so a window of kRegWin diagonals (slots of 32, lane = offset in the
+// slot) holds whole wavefronts while that bound stays inside it. Each lane keeps the M,
+// I and D values of its diagonals for the last scores the recurrence looks back to
+// (X, O + E and E, in steps of g = gcd(X, O, E)) in shift registers; neighbour diagonals
+// k - 1 and k + 1 come from the adjacent lane by shuffle. Cells are computed exactly as
+// in wfa_affine_group (candidate order, strict >, validity), so values, ops and the end
+// cell are identical; only the traceback's aux words go to memory, in the same history
+// layout (one row of kRegWin words per layer and score), so the same traceback runs.
+// A pair whose reachable band would leave the window stops and is redone by
+// wfa_affine_group.
+// Slots of 32 diagonals, centred on diagonal 0 so that the band of the early scores (and
+// of most pairs' whole search) is one slot: 0 = [-16, 15], 1 = [-48, -17], 2 = [16, 47],
+// 3 = [-80, -49], 4 = [48, 79].
+constexpr int kRegSlots = 5;
+constexpr int kRegMaxLen = 1024;  // qlen + tlen below which a pair tries the register kernel
+constexpr int kRegWin = 32 * kRegSlots;
+constexpr int kRegLo = -kRegWin / 2;
+__host__ __device__ constexpr int reg_slot_lo(int h) { return h == 0 ? -16 : h == 1 ? -48 : h == 2 ? 16 : h == 3 ? -80 : 48; }
+__host__ __device__ constexpr int reg_left(int h) { return h == 0 ? 1 : h == 1 ? 3 : h == 2 ? 0 : h == 4 ? 2 : -1; }
+__host__ __device__ constexpr int reg_right(int h) { return h == 0 ? 2 : h == 1 ? 0 : h == 2 ? 4 : h == 3 ? 1 : -1; }
+
+// value at diagonal k - 1 (UP) or k + 1 of slot h, across lanes and into the adjacent slot
+template <bool UP>
+__device__ __forceinline__ int32_t reg_neighbor(const int32_t (&v)[kRegSlots], int h) {
+    const int lane = lane_id();
+    if (UP) {
+        const int32_t a = __shfl_up_sync(PHR_FULL_MASK, v[h], 1);
+        const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_left(h) >= 0 ? v[reg_left(h)] : UNSET, 31);
+        return lane == 0 ? b : a;
+    }
+    const int32_t a = __shfl_down_sync(PHR_FULL_MASK, v[h], 1);
+    const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_right(h) >= 0 ? v[reg_right(h)] : UNSET, 0);
+    return lane == 31 ? b : a;
+}
+
+template <class S, int XS, int OES, int ES>
+__device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
+                               uint64_t region_bytes) {
+    constexpr int RM = (XS > OES ? XS : OES);  // M values kept: steps 1..RM back
+    const int lane = lane_id();
+    const int qn = d.qn, tn = d.tn;
+    const bool fitting = tn > qn + qn / 2 + 10;
+    const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
+    const int g = X / XS;  // the step of reachable scores
+    const uint32_t* qb = seq_base<S>(P, d.q_word);
+    const uint32_t* tb = seq_base<S>(P, d.t_word);
+    const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
+
+    // region: [runs][aux rows: kRegWin words per layer per visited score]; row r holds
+    // score r * g, so the traceback needs no directory
+    uint32_t* runs = reinterpret_cast<uint32_t*>(region);
+    const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
+    const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
+    const uint64_t row_cap = rest / (3 * kRegWin * 4);
+    uint32_t* auxs = reinterpret_cast<uint32_t*>(region + runs_bytes);
+    const int wlo = max(kRegLo, -tn), whi = min(kRegLo + kRegWin - 1, qn);  // window clipped to [-tn, qn]
+
+    int32_t M[RM][kRegSlots], I[ES][kRegSlots], D[ES][kRegSlots];
+#pragma unroll
+    for (int h = 0; h < kRegSlots; ++h) {
+#pragma unroll
+        for (int r = 0; r < RM; ++r) M[r][h] = UNSET;
+#pragma unroll
+        for (int r = 0; r < ES; ++r) {
+            I[r][h] = UNSET;
+            D[r][h] = UNSET;
+        }
+    }
+    uint32_t wf_cells = 0, lcp_words = 0;
+    bool done = false, overflow = row_cap < 2;
+    int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
+    // ---- s = 0: M[0][0] = extend(0, 0), at slot -kRegLo / 32, lane 0 ----
+    int32_t v0 = 0;
+    if (!overflow) {
+        if (lane == 0) v0 = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
+        v0 = __shfl_sync(PHR_FULL_MASK, v0, 0);
+        if (lane == 0) auxs[-kRegLo] = 0;  // row 0 = score 0, diagonal 0
+        if (lane == 16) M[0][0] = v0;  // diagonal 0: slot 0, lane 16
+        if (!fitting) {
+            if (qn - tn == 0 && v0 == qn) done = true, t_end = tn;
+        } else if (qn <= tn && v0 == qn) {
+            done = true;
+            t_end = qn;
+        }
+    }
+    uint64_t row = 1;
+    int64_t s = g;
+    // half-width of the reachable band, floor((s - O) / E) from score O + E on, kept
+    // incrementally; `active` marks the slots the band has reached (they stay reached)
+    int hw = 0;
+    int64_t next_hw = static_cast<int64_t>(O) + E;
+    uint32_t active = 1u;
+    for (; !done && !overflow && s <= hard_max_s; s += g) {
+        // reachable diagonals of this score; leaving the window ends this kernel's attempt
+        while (s >= next_hw) {
+            ++hw;
+            next_hw += E;
+        }
+        const int blo = max(-tn, -hw);
+        const int bhi = min(qn, hw);
+        if (blo < wlo || bhi > whi || row >= row_cap) {
+            overflow = true;
+            break;
+        }
+        if (lane == 0) wf_cells += static_cast<uint32_t>(bhi - blo + 1);
+        uint32_t* arow = auxs + row * (3 * kRegWin);
+        int32_t nM[kRegSlots], nI[kRegSlots], nD[kRegSlots];
+        int best_k = INT32_MAX, best_l = 0;
+#pragma unroll
+        for (int h = 0; h < kRegSlots; ++h) {
+            nM[h] = nI[h] = nD[h] = UNSET;
+            const int klo = reg_slot_lo(h);
+            if (klo + 31 < blo || klo > bhi) continue;  // warp-uniform: slot outside the band
+            active |= 1u << h;
+            const int k = klo + lane;
+            const int32_t mo_dn = reg_neighbor<true>(M[OES - 1], h);   // M[s - O - E][k - 1]
+            const int32_t ie_dn = reg_neighbor<true>(I[ES - 1], h);    // I[s - E][k - 1]
+            const int32_t mo_up = reg_neighbor<false>(M[OES - 1], h);  // M[s - O - E][k + 1]
+            const int32_t de_up = reg_neighbor<false>(D[ES - 1], h);   // D[s - E][k + 1]
+            // I (wfa_simd.rs:682-738): [open from M, extend I], strict >
+            int32_t ins = UNSET;
+            uint32_t iop = 0;
+            if (pos_ok(mo_dn + 1, k, qn, tn)) ins = mo_dn + 1;
+            if (pos_ok(ie_dn + 1, k, qn, tn) && ie_dn + 1 > ins) {
+                ins = ie_dn + 1;
+                iop = 1;
             }
-            const AffDir e = dir_at(ss);
-            if (layer == 0) {
-                const uint32_t aux = auxs[e.L[0].base + (k - e.L[0].lo)];
-                const uint32_t mop = aux & 3;
-                const int32_t raw = static_cast<int32_t>(aux >> 2);
-                const int mc = max(qi - raw, 0);
-                if (mc > 0) {
-                    rw.push(0, static_cast<uint32_t>(mc));
-                    qi -= mc;
-                    ti -= mc;
+            int32_t del = UNSET;
+            uint32_t dop = 0;
+            if (pos_ok(mo_up, k, qn, tn)) del = mo_up;
+            if (pos_ok(de_up, k, qn, tn) && de_up > del) {
+                del = de_up;
+                dop = 1;
+            }
+            // M (wfa_simd.rs:743-765): [mismatch-extend, ins close, del close], strict >
+            int32_t best = UNSET;
+            uint32_t mop = 0;
+            if (pos_ok(M[XS - 1][h] + 1, k, qn, tn)) best = M[XS - 1][h] + 1;
+            if (pos_ok(ins, k, qn, tn) && ins > best) {
+                best = ins;
+                mop = 1;
+            }
+            if (pos_ok(del, k, qn, tn) && del > best) {
+                best = del;
+                mop = 2;
+            }
+            int32_t mval = UNSET;
+            uint32_t aux = 0;
+            if (best != UNSET) {
+                mval = extend_valid<S>(qb, qn, tb, tn, best, k, lcp_words);
+                aux = (static_cast<uint32_t>(best) << 2) | mop;
+            }
+            nM[h] = mval;
+            nI[h] = ins;
+            nD[h] = del;
+            arow[k - kRegLo] = aux;
+            arow[kRegWin + k - kRegLo] = iop;
+            arow[2 * kRegWin + k - kRegLo] = dop;
+            // end cell: value == qn in layer order m, ins, del; smallest k (largest t_end)
+            const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
+            const bool cand = layer >= 0 && (fitting ? k >= qn - tn : k == qn - tn);
+            const unsigned bal = __ballot_sync(PHR_FULL_MASK, cand);
+            if (bal) {
+                const int src = __ffs(bal) - 1;
+                const int l = __shfl_sync(PHR_FULL_MASK, layer, src);
+                if (klo + src < best_k) {
+                    best_k = klo + src;
+                    best_l = l;
                 }
-                if (mop == 0) {
-                    rw.push(1, 1);
-                    --qi;
-                    --ti;
-                    ++n_edit;
-                    ss -= X;
-                } else {
-                    layer = static_cast<int>(mop);
-                }
-            } else if (layer == 1) {
-                rw.push(3, 1);  // ins (query-extra) -> 'D'
-                --qi;
-                ++n_edit;
-                if (auxs[e.L[1].base + (k - e.L[1].lo)] == 0) {
-                    ss -= O + E;
-                    layer = 0;
-                } else {
-                    ss -= E;
-                }
-                k -= 1;
-            } else {
-                rw.push(2, 1);  // del (target-extra) -> 'I'
-                --ti;
-                ++n_edit;
-                if (auxs[e.L[2].base + (k - e.L[2].lo)] == 0) {
-                    ss -= O + E;
-                    layer = 0;
-                } else {
-                    ss -= E;
-                }
-                k += 1;
             }
         }
-        if (guard < 0) atomicOr(P.error_flag, 4u);
-        rw.flush();
+        // shift the histories of the reached slots: this score becomes one step back
+#pragma unroll
+        for (int h = 0; h < kRegSlots; ++h) {
+            if (!((active >> h) & 1u)) continue;
+#pragma unroll
+            for (int r = RM - 1; r > 0; --r) M[r][h] = M[r - 1][h];
+            M[0][h] = nM[h];
+#pragma unroll
+            for (int r = ES - 1; r > 0; --r) {
+                I[r][h] = I[r - 1][h];
+                D[r][h] = D[r - 1][h];
+            }
+            I[0][h] = nI[h];
+            D[0][h] = nD[h];
+        }
+        ++row;  // the traceback addresses row s / g directly (no directory)
+        if (best_k != INT32_MAX) {
+            done = true;
+            s_end = static_cast<int>(s);
+            t_end = qn - best_k;
+            k_end = best_k;
+            layer_end = best_l;
+        }
     }
-    const int leader = lane_id() & ~(G - 1);
-    const uint32_t nr = __shfl_sync(PHR_FULL_MASK, rw.n, leader);
-    const bool ovf = __shfl_sync(PHR_FULL_MASK, rw.overflow ? 1 : 0, leader) != 0;
-    const uint32_t ned = __shfl_sync(PHR_FULL_MASK, n_edit, leader);
+    {
+        const unsigned lw = __reduce_add_sync(PHR_FULL_MASK, lcp_words);
+        if (lane == 0 && P.work) {
+            atomicAdd(P.work + 2, static_cast<unsigned long long>(wf_cells));
+            atomicAdd(P.work + 3, static_cast<unsigned long long>(lw));
+        }
+    }
+    if (overflow) {
+        // redo with wfa_affine_group, which sizes its bands per score
+        if (lane == 0) report_redo(P, pid, wfa_region_est(qn, tn, true));
+        return;
+    }
     __syncwarp();
-    const uint32_t nr_fmt = (trace && !ovf) ? nr : 0;
-    char* out = act ? P.text + P.text_off[pid] : nullptr;
-    const uint32_t tl = format_group(runs, nr_fmt, out, G);
-    if (act && gl == 0) {
-        if (trace && !ovf) {
-            PairOut o;
-            o.status = PHR_OK;
-            o.ed = static_cast<int32_t>(ned);  // levenshtein_from_cigar: X + I/D lengths
-            o.t_consumed = t_end;
-            o.affine_score = s_end;
-            o.n_runs = nr;
-            o.text_len = tl;
-            P.out[pid] = o;
-        } else if (failed) {
-            PairOut o = {};
-            o.status = PHR_ALIGNMENT_FAILED;
-            P.out[pid] = o;
-        } else if (trace && ovf) {
-            atomicOr(P.error_flag, 2u);
-        }
-    }
+    affine_finish(P, pid, true, 32, qn, tn, X, O, E, runs, auxs, nullptr, done, !done, s_end, t_end, k_end,
+                  layer_end, g, kRegWin, kRegLo);
 }
 
 // Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
 constexpr int kAffWarpSmem = kAffRingGroups * kAffRing * static_cast<int>(sizeof(SDir)) + kWarpSeqWords * 4;
 
 template <class S, bool kAffine>
-__global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams P) {
+__global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams P) {
     extern __shared__ __align__(16) uint8_t wfa_smem[];
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -1061,6 +1296,21 @@ __global__ void __launch_bounds__(256, kAffine ? 3 : 4) wfa_kernel(ExtendParams 
         if (!P.task_off && P.task_need && P.task_need[task] > slot_bytes) {
             if (act && (lane & (G - 1)) == 0) report_redo(P, pid, P.task_need[task] / (32 / G));
             continue;
+        }
+        if constexpr (kAffine && S::kBits == 2) {
+            // short 2-bit pairs of one warp each, costs with a register specialisation:
+            // wavefronts in registers (redo passes and wide bands take the group kernel)
+            if (G == 32 && !P.task_off && act && d.qn + d.tn < kRegMaxLen) {
+                const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
+                if (X == 4 && O == 6 && E == 2) {
+                    wfa_affine_reg<S, 2, 4, 1>(P, d, pid, region, region_bytes);
+                    continue;
+                }
+                if (X == 2 && O == 4 && E == 1) {
+                    wfa_affine_reg<S, 2, 5, 1>(P, d, pid, region, region_bytes);
+                    continue;
+                }
+            }
         }
         if (kAffine) {
             // per warp: one directory ring per group of >= 4 lanes, then the sequence words
