@@ -479,16 +479,13 @@ phr_status phr_extend_batch_device(phr_ctx* c, phr_engine engine, const phr_pair
     cudaSetDevice(ctx->device);
     if (!batch || !out) return phr::set_error(ctx, PHR_ERR_ARG, "NULL batch/arena");
     if (!valid_engine(engine)) return phr::set_error(ctx, PHR_ERR_ARG, "unknown engine");
-    // sum of lengths (device arrays): one reduction pass on the host copy of lengths
+    // sum of lengths (device arrays): one reduction kernel
     const uint64_t n = batch->n_pairs;
     out->cigar_used = 0;
     if (n == 0) return PHR_OK;
-    std::vector<uint32_t> ql(n), tl(n);
-    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(ql.data(), batch->q_len, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(tl.data(), batch->t_len, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    uint64_t sum_qt = 0;
-    for (uint64_t i = 0; i < n; ++i) sum_qt += static_cast<uint64_t>(ql[i]) + tl[i];
+    cudaError_t e = cudaSuccess;
+    const uint64_t sum_qt = phr::device_length_sum(ctx, batch->q_len, batch->t_len, n, &e);
+    if (e != cudaSuccess) return phr::cuda_status(ctx, e, "length sum");
     phr::DevPairs dp;
     dp.n = n;
     dp.seq = batch->seq;

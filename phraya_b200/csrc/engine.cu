@@ -563,6 +563,41 @@ inline unsigned blocks_for(uint64_t n, unsigned t) { return static_cast<unsigned
 
 }  // namespace
 
+namespace {
+__global__ void sum_lengths_kernel(const uint32_t* a, const uint32_t* b, uint64_t n, unsigned long long* out) {
+    unsigned long long acc = 0;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        acc += static_cast<unsigned long long>(a[i]) + b[i];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(PHR_FULL_MASK, acc, o);
+    if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+}  // namespace
+
+uint64_t device_length_sum(Ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, cudaError_t* err) {
+    *err = cudaSuccess;
+    if (!ctx->d_counters) {
+        *err = cudaMalloc(&ctx->d_counters, 256);
+        if (*err != cudaSuccess) return 0;
+    }
+    if (!ctx->h_pinned) {
+        *err = cudaMallocHost(&ctx->h_pinned, 256);
+        if (*err != cudaSuccess) return 0;
+    }
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(ctx->d_counters);
+    unsigned long long* h = static_cast<unsigned long long*>(ctx->h_pinned);
+    cudaStream_t st = ctx->stream;
+    if ((*err = cudaMemsetAsync(d, 0, 8, st)) != cudaSuccess) return 0;
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 4ull * ctx->sm_count));
+    {
+        KernelScope ks(ctx, "sum_lengths");
+        sum_lengths_kernel<<<std::max(1u, grid), 256, 0, st>>>(a, b, n, d);
+    }
+    if ((*err = cudaMemcpyAsync(h, d, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return 0;
+    if ((*err = cudaStreamSynchronize(st)) != cudaSuccess) return 0;
+    return *h;
+}
+
 size_t extend_arena_need(uint64_t n, uint64_t seq_bytes, uint64_t sum_qt) {
     size_t s = 0;
     auto add = [&](size_t b) { s += (b + 511) / 256 * 256; };

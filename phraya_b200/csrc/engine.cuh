@@ -144,6 +144,9 @@ struct DevResults {
 phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& pairs, phr_affine_costs costs,
                       DevResults* out, uint64_t sum_qt_len);
 
+// Sum of a[i] + b[i] over device arrays of n lengths (one reduction kernel, 8 bytes back).
+uint64_t device_length_sum(Ctx* ctx, const uint32_t* a, const uint32_t* b, uint64_t n, cudaError_t* err);
+
 // Upper bound of the device arena bytes run_extend needs for a batch.
 size_t extend_arena_need(uint64_t n, uint64_t seq_bytes, uint64_t sum_qt_len);
 
