@@ -421,6 +421,86 @@ phr_status phr_align_reads(phr_ctx* ctx, const phr_index* idx, const phr_read_ba
                            phr_align_stats* stats);
 
 /* ------------------------------------------------------------------------- */
+/* Variant observations and coverage of the aligned reads                    */
+/* (phraya-align/src/executor.rs:735-775, 814-1096)                           */
+/* ------------------------------------------------------------------------- */
+
+/*
+ * One VariantObservation (phraya-core/src/types.rs:217-283) as extract_variants_from_cigar
+ * (executor.rs:814-1046) builds it from a read's primary alignment. The per-read fields
+ * the device does not know -- mapq, avg_base_quality, provenance, the CIGAR string
+ * (the read's primary CIGAR) and mate information -- are the host's, shared by every
+ * variant of read `read`.
+ */
+typedef struct {
+    uint32_t position;               /* 0-based reference position                     */
+    uint8_t ref_base;                /* '.' for an insertion                           */
+    uint8_t variant_type;            /* VariantType: 0 SNP, 1 insertion, 2 deletion    */
+    uint8_t in_tandem_repeat;        /* is_in_repeat_region (executor.rs:806-809)       */
+    uint8_t strand;                  /* 0 forward, 1 reverse complement                */
+    uint32_t read;                   /* index of the read in its batch                 */
+    uint32_t edit_distance;          /* the primary alignment's                        */
+    double confidence;               /* kmer_uniqueness * (1 - ed / max(|q|, 1))        */
+    double kmer_uniqueness;          /* 0 inside a hotspot interval (is_in_hotspot), 1  */
+    uint64_t coverage_off;           /* local_coverage = coverage[off .. off + len)     */
+    uint32_t coverage_len;
+    uint32_t coverage_variant_offset;/* index of `position` within local_coverage       */
+    uint64_t allele_off;             /* all_alleles = alleles[off .. off + n), ascending */
+    uint32_t n_alleles;
+    uint32_t _pad;
+} phr_variant;
+
+typedef struct {
+    uint8_t base;                    /* allele byte ('.' = deleted)                    */
+    uint8_t _pad[3];
+    uint32_t count;
+} phr_allele;
+
+typedef struct {
+    uint32_t coverage_radius;        /* 0: the strategy's (AlignConfig, executor.rs:124-128:
+                                        Fast 150, Balanced 50, Sensitive 25)             */
+    uint32_t _pad;
+    const uint32_t* hotspot_start;   /* plan.hotspot_intervals: sorted, non-overlapping */
+    const uint32_t* hotspot_end;     /* [start, end) intervals, host arrays; may be NULL */
+    uint64_t n_hotspots;
+} phr_variant_config;
+
+typedef struct {
+    uint64_t* read_variant_off;      /* n_reads + 1 entries: read i's variants are
+                                        variants[off[i] .. off[i + 1])                 */
+    phr_variant* variants;
+    uint64_t variant_capacity;
+    uint64_t variant_used;
+    uint32_t* coverage;
+    uint64_t coverage_capacity;
+    uint64_t coverage_used;
+    phr_allele* alleles;
+    uint64_t allele_capacity;
+    uint64_t allele_used;
+} phr_variant_arena;
+
+/*
+ * phr_align_reads plus, for every read with a result, the variant observations of its
+ * primary alignment on the device: local coverage is the read's raw windowed coverage
+ * (compute_windowed_coverage, executor.rs:1071-1090: one window per alignment, primary
+ * then alternatives, count 1 over [target_start, target_end)), in_tandem_repeat comes
+ * from the index's tandem-repeat regions (detect_tandem_repeats with
+ * min_repeat_count 3, phraya-core/src/lib.rs:79-135). The coverage track the reference
+ * stores per read is each alignment's span with quantize_coverage(1) = 0
+ * (executor.rs:1092-1096), i.e. derived from the alignments alone.
+ */
+phr_status phr_align_reads_variants(phr_ctx* ctx, const phr_index* idx, const phr_read_batch* reads,
+                                    const phr_align_config* cfg, phr_read_result_arena* out,
+                                    const phr_variant_config* vcfg, phr_variant_arena* vout,
+                                    phr_align_stats* stats);
+
+/* The index's tandem-repeat regions (TargetContext::build, executor.rs:440): region r
+ * covers [start[r], end[r]] (end inclusive, RepeatRegion, phraya-core/src/lib.rs:10-18).
+ * Writes min(n, cap) regions and the total count in *n. */
+phr_status phr_index_repeat_regions(const phr_index* idx, uint32_t* start, uint32_t* end, uint64_t cap,
+                                    uint64_t* n);
+
+/* ------------------------------------------------------------------------- */
 /* Serving loop: device-resident index, admission by free HBM, continuous    */
 /* batching. No counterpart in the reference (its CLI is batch-only).         */
 /* ------------------------------------------------------------------------- */

@@ -65,6 +65,12 @@ def lib():
         L.orc_align_reads.restype = C.c_int32
         L.orc_align_reads.argtypes = [C.c_void_p, C.POINTER(A.ReadBatch), C.POINTER(A.AlignConfig),
                                       C.POINTER(A.ReadResultArena), C.POINTER(A.AlignStats), C.c_int32]
+        L.orc_tandem_repeats.restype = C.c_uint64
+        L.orc_tandem_repeats.argtypes = [C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_uint64]
+        L.orc_variants.restype = C.c_int32
+        L.orc_variants.argtypes = [C.c_void_p, C.POINTER(A.ReadBatch), C.POINTER(A.ReadResultArena),
+                                   C.POINTER(A.AlignConfig), C.POINTER(A.VariantConfig),
+                                   C.POINTER(A.VariantArena)]
         _lib = L
     return _lib
 
@@ -73,7 +79,8 @@ def default_threads():
     return max(1, os.cpu_count() or 1)
 
 
-from phraya_b200.batch import PackedPairs, PackedReads, ALN_DTYPE, READ_RESULT_DTYPE  # noqa: E402
+from phraya_b200.batch import (PackedPairs, PackedReads, ALN_DTYPE, READ_RESULT_DTYPE,  # noqa: E402
+                               VARIANT_DTYPE, ALLELE_DTYPE)
 
 
 def _unpack_results(n, aln, cig):
@@ -199,6 +206,44 @@ def score_alignments(alns, query_len):
     return int(pi[0]), [i for i in range(n) if alt[i]]
 
 
+def tandem_repeats(seq):
+    """detect_tandem_repeats with min_repeat_count 3 -> [(start, end_inclusive), ...]."""
+    seq = bytes(seq)
+    cap = max(1, len(seq) // 6 + 1)
+    st = np.zeros(cap, dtype=np.uint32)
+    en = np.zeros(cap, dtype=np.uint32)
+    n = int(lib().orc_tandem_repeats(seq, len(seq), st.ctypes.data, en.ctypes.data, cap))
+    assert n <= cap
+    return [(int(a), int(b)) for a, b in zip(st[:n], en[:n])]
+
+
+def variant_config(radius=0, hotspots=()):
+    """-> (VariantConfig, keep-alive arrays). hotspots: sorted [(start, end), ...]."""
+    hs = np.array([h[0] for h in hotspots], dtype=np.uint32)
+    he = np.array([h[1] for h in hotspots], dtype=np.uint32)
+    vc = A.VariantConfig(radius, 0, hs.ctypes.data if len(hs) else None, he.ctypes.data if len(he) else None,
+                         len(hs))
+    return vc, (hs, he)
+
+
+def unpack_variants(n, off, var, cov, al):
+    """-> per read [(position, ref, type, in_repeat, strand, ed, confidence, kmer, coverage list,
+    variant_offset, [(allele, count), ...]), ...]"""
+    out = []
+    for i in range(n):
+        rows = []
+        for v in var[int(off[i]):int(off[i + 1])]:
+            c0 = int(v["coverage_off"])
+            a0 = int(v["allele_off"])
+            rows.append((int(v["position"]), int(v["ref_base"]), int(v["variant_type"]), int(v["in_tandem_repeat"]),
+                         int(v["strand"]), int(v["edit_distance"]), float(v["confidence"]),
+                         float(v["kmer_uniqueness"]), cov[c0:c0 + int(v["coverage_len"])].tolist(),
+                         int(v["coverage_variant_offset"]),
+                         [(int(a["base"]), int(a["count"])) for a in al[a0:a0 + int(v["n_alleles"])]]))
+        out.append(rows)
+    return out
+
+
 def unpack_read_results(n, rr, aln, cig):
     """-> [(outcome, has_result, reverse, [(cigar, ed, qs, qe, ts, te), ...])]"""
     out = []
@@ -248,6 +293,31 @@ class Target:
             raise RuntimeError(f"orc_align_reads failed: {rc}")
         st = (stats.placed, stats.no_seed, stats.below_threshold, stats.fast_cutoff, stats.no_alignment)
         return rr, aln[:arena.aln_used], cig[:arena.cigar_used], st
+
+    def variants_packed(self, packed, rr, aln, cig, strategy=A.BALANCED, radius=0, hotspots=()):
+        """Variant observations (executor.rs:735-775) from align results in phr_align_reads layout.
+        Returns (read_variant_off, variants, coverage, alleles) ndarrays."""
+        n = packed.n
+        off = np.zeros(n + 1, dtype=np.uint64)
+        vcap = int(sum(len(bytes(cig[a["cigar_off"]:a["cigar_off"] + a["cigar_len"]])) for a in aln)) + 16
+        var = np.zeros(vcap, dtype=VARIANT_DTYPE)
+        r = radius or {A.FAST: 150, A.BALANCED: 50}.get(strategy, 25)
+        ccap = vcap * (2 * r + 1) + 16
+        cov = np.zeros(ccap, dtype=np.uint32)
+        acap = int(packed.len.sum()) + vcap + 16
+        al = np.zeros(acap, dtype=ALLELE_DTYPE)
+        arena = A.VariantArena(off.ctypes.data, var.ctypes.data, vcap, 0, cov.ctypes.data, ccap, 0, al.ctypes.data,
+                               acap, 0)
+        res = A.ReadResultArena(rr.ctypes.data, aln.ctypes.data, len(aln), len(aln), cig.ctypes.data, len(cig),
+                                len(cig))
+        vc, keep = variant_config(radius, hotspots)
+        cfg = A.AlignConfig(strategy, A.GAP_AFFINE)
+        b = packed.batch()
+        rc = lib().orc_variants(self._t, C.byref(b), C.byref(res), C.byref(cfg), C.byref(vc), C.byref(arena))
+        if rc != 0:
+            raise RuntimeError(f"orc_variants failed: {rc}")
+        del keep
+        return off, var[:arena.variant_used], cov[:arena.coverage_used], al[:arena.allele_used]
 
     def align_reads(self, reads, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, stored=None, nthreads=None):
         packed = PackedReads(reads, stored)

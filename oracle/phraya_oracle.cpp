@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -1092,10 +1093,18 @@ std::vector<uint8_t> revcomp(const uint8_t* s, size_t n) {
     return out;
 }
 
+// RepeatRegion (phraya-core/src/lib.rs:10-18) without its period/unit strings.
+struct RepeatRegionT {
+    size_t start, end;  // end inclusive
+};
+
+std::vector<RepeatRegionT> detect_tandem_repeats(const uint8_t* seq, size_t n, size_t min_count);
+
 struct Target {
     std::vector<uint8_t> bytes;
     Index index;
     int alphabet = PHR_ALPHABET_DNA;
+    std::vector<RepeatRegionT> repeats;  // TargetContext::repeat_regions (executor.rs:440-441)
 };
 
 size_t chain_cap(int strategy) { return strategy == PHR_FAST ? 1 : strategy == PHR_BALANCED ? 2 : 50; }
@@ -1237,6 +1246,151 @@ void parallel_for(uint64_t n, int nthreads, F&& fn) {
             }
         });
     for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------------------
+// Tandem repeats and variant observations
+//   detect_tandem_repeats        phraya-core/src/lib.rs:79-135 (RepeatDetectorConfig
+//                                default min_repeat_count 3, lib.rs:40-52)
+//   is_in_repeat_region          phraya-align/src/executor.rs:806-809
+//   is_in_hotspot                executor.rs:795-798
+//   compute_windowed_coverage    executor.rs:1071-1090, WindowedCoverage::get_abs :190-197,
+//                                get_abs_multi :218-220
+//   extract_variants_from_cigar  executor.rs:814-1046, parse_cigar :1048-1061
+//   call site / confidence       executor.rs:735-775 (primary_score = 1 - ed / max(|q|, 1))
+// ---------------------------------------------------------------------------
+std::vector<RepeatRegionT> detect_tandem_repeats(const uint8_t* seq, size_t n, size_t min_count) {
+    std::vector<uint8_t> up(seq, seq + n);  // sequence.to_uppercase() (ASCII)
+    for (uint8_t& c : up)
+        if (c >= 'a' && c <= 'z') c = static_cast<uint8_t>(c - 32);
+    std::vector<RepeatRegionT> regions;
+    if (n < min_count * 2) return regions;
+    size_t cur = 0;
+    while (cur + min_count * 2 <= n) {
+        bool found = false;
+        for (size_t period = 4; period >= 2; --period) {  // (2..=4).rev()
+            if (cur + period * min_count > n) continue;
+            size_t count = 1, end = cur + period;
+            while (end + period <= n && std::memcmp(&up[cur], &up[end], period) == 0) {
+                ++count;
+                end += period;
+            }
+            if (count >= min_count) {
+                regions.push_back({cur, end - 1});
+                cur = end;
+                found = true;
+                break;
+            }
+        }
+        if (!found) ++cur;
+    }
+    return regions;
+}
+
+// Last region whose start <= pos; inside when pos < its (inclusive) end, as the reference.
+bool in_repeat_region(size_t pos, const std::vector<RepeatRegionT>& r) {
+    size_t lo = 0, hi = r.size();
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (r[mid].start <= pos) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo > 0 && pos < r[lo - 1].end;
+}
+
+bool in_hotspot(uint32_t pos, const uint32_t* hs, const uint32_t* he, size_t n) {
+    size_t lo = 0, hi = n;
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (hs[mid] <= pos) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo > 0 && pos < he[lo - 1];
+}
+
+struct VariantOut {
+    std::vector<phr_variant> v;
+    std::vector<uint32_t> cov;
+    std::vector<phr_allele> al;
+};
+
+// extract_variants_from_cigar for one read; windows = the read's coverage windows.
+void extract_variants(const std::string& cigar, size_t target_start, const uint8_t* query, size_t qlen,
+                      const uint8_t* target, size_t tlen, uint32_t ed,
+                      const std::vector<std::pair<size_t, size_t>>& windows,
+                      const std::vector<RepeatRegionT>& reps, const uint32_t* hs, const uint32_t* he, size_t nhs,
+                      double primary_score, size_t radius, uint8_t strand, uint32_t read, VariantOut* out) {
+    auto cov_at = [&](size_t pos) {  // get_abs_multi
+        uint32_t c = 0;
+        for (auto& w : windows)
+            if (pos >= w.first && pos < w.second) c += 1;
+        return c;
+    };
+    auto emit = [&](size_t tp, uint8_t ref, uint8_t type, const std::vector<std::pair<uint8_t, uint32_t>>& alleles) {
+        phr_variant o;
+        std::memset(&o, 0, sizeof(o));
+        const size_t ws = tp >= radius ? tp - radius : 0;
+        const size_t we = std::min(tp + radius + 1, tlen);
+        o.coverage_off = out->cov.size();
+        for (size_t p = ws; p < we; ++p) out->cov.push_back(cov_at(p));
+        o.coverage_len = static_cast<uint32_t>(we > ws ? we - ws : 0);
+        o.coverage_variant_offset = static_cast<uint32_t>(tp - ws);
+        o.position = static_cast<uint32_t>(tp);
+        o.ref_base = ref;
+        o.variant_type = type;
+        o.in_tandem_repeat = in_repeat_region(tp, reps) ? 1 : 0;
+        o.strand = strand;
+        o.read = read;
+        o.edit_distance = ed;
+        o.kmer_uniqueness = in_hotspot(static_cast<uint32_t>(tp), hs, he, nhs) ? 0.0 : 1.0;
+        o.confidence = o.kmer_uniqueness * primary_score;
+        o.allele_off = out->al.size();
+        for (auto& a : alleles) {
+            phr_allele x;
+            std::memset(&x, 0, sizeof(x));
+            x.base = a.first;
+            x.count = a.second;
+            out->al.push_back(x);
+        }
+        o.n_alleles = static_cast<uint32_t>(alleles.size());
+        out->v.push_back(o);
+    };
+    size_t q = 0, t = target_start;
+    size_t i = 0;
+    while (i < cigar.size()) {
+        size_t count = 0;
+        bool digits = false;
+        while (i < cigar.size() && cigar[i] >= '0' && cigar[i] <= '9') {
+            count = count * 10 + static_cast<size_t>(cigar[i] - '0');
+            ++i;
+            digits = true;
+        }
+        if (i >= cigar.size()) break;
+        const char op = cigar[i++];
+        if (!digits) count = 1;  // count_str.parse().unwrap_or(1)
+        if (op == 'M') {
+            q += count;
+            t += count;
+        } else if (op == 'X') {
+            for (size_t k = 0; k < count; ++k) {
+                const size_t qp = q + k, tp = t + k;
+                if (qp < qlen && tp < tlen) emit(tp, target[tp], 0, {{query[qp], 1u}});
+            }
+            q += count;
+            t += count;
+        } else if (op == 'I') {  // target-extra: deletion, ref = first deleted base, allele '.'
+            if (t < tlen && q < qlen) emit(t, target[t], 2, {{static_cast<uint8_t>('.'), 1u}});
+            t += count;
+        } else if (op == 'D') {  // query-extra: insertion at t, alleles = inserted bases
+            if (q < qlen && t < tlen) {
+                std::map<uint8_t, uint32_t> m;
+                for (size_t k = q; k < std::min(q + count, qlen); ++k) m[query[k]] += 1;
+                std::vector<std::pair<uint8_t, uint32_t>> al(m.begin(), m.end());
+                emit(t, static_cast<uint8_t>('.'), 1, al);
+            }
+            q += count;
+        }
+    }
 }
 
 }  // namespace
@@ -1409,6 +1563,7 @@ void* orc_target_create(const uint8_t* target, uint64_t len, int32_t alphabet) {
     else
         sketch_seq(target, static_cast<int64_t>(len), 6, 5, PHR_ALPHABET_PROTEIN, &sk);
     build_index(sk, 256, &tg->index);
+    tg->repeats = detect_tandem_repeats(target, len, 3);
     return tg;
 }
 
@@ -1463,6 +1618,65 @@ int32_t orc_align_reads(void* tgt, const phr_read_batch* reads, const phr_align_
     }
     out->aln_used = aused;
     out->cigar_used = cused;
+    return PHR_OK;
+}
+
+// Tandem repeats of `s` (min_repeat_count 3). Writes min(count, cap) regions; returns the count.
+uint64_t orc_tandem_repeats(const uint8_t* s, uint64_t n, uint32_t* start, uint32_t* end, uint64_t cap) {
+    std::vector<RepeatRegionT> r = detect_tandem_repeats(s, n, 3);
+    for (uint64_t i = 0; i < r.size() && i < cap; ++i) {
+        start[i] = static_cast<uint32_t>(r[i].start);
+        end[i] = static_cast<uint32_t>(r[i].end);
+    }
+    return r.size();
+}
+
+// Variant observations of every read with a result in `res` (the layout phr_align_reads
+// writes: primary first, then the alternatives), as align_read builds them
+// (executor.rs:735-775). Output layout matches phr_align_reads_variants. Returns 0 or
+// PHR_ERR_CAPACITY.
+int32_t orc_variants(void* tgt, const phr_read_batch* reads, const phr_read_result_arena* res,
+                     const phr_align_config* cfg, const phr_variant_config* vcfg, phr_variant_arena* vout) {
+    const Target& tg = *static_cast<Target*>(tgt);
+    const uint64_t n = reads->n_reads;
+    size_t radius = vcfg && vcfg->coverage_radius ? vcfg->coverage_radius
+                    : cfg->strategy == PHR_FAST   ? 150
+                    : cfg->strategy == PHR_BALANCED ? 50
+                                                    : 25;
+    const uint32_t* hs = vcfg ? vcfg->hotspot_start : nullptr;
+    const uint32_t* he = vcfg ? vcfg->hotspot_end : nullptr;
+    const size_t nhs = vcfg && hs && he ? vcfg->n_hotspots : 0;
+    const size_t tlen = tg.bytes.size();
+    VariantOut out;
+    for (uint64_t i = 0; i < n; ++i) {
+        vout->read_variant_off[i] = out.v.size();
+        const phr_read_result& r = res->reads[i];
+        if (!r.has_result || r.n_aln == 0) continue;
+        const uint8_t* read = reads->seq + reads->off[i];
+        const size_t qlen = reads->len[i];
+        std::vector<uint8_t> q = r.reverse ? revcomp(read, qlen) : std::vector<uint8_t>(read, read + qlen);
+        std::vector<std::pair<size_t, size_t>> windows;
+        for (uint32_t a = 0; a < r.n_aln; ++a) {
+            const phr_alignment& x = res->aln[r.aln_off + a];
+            const size_t s0 = std::min<size_t>(x.target_start, tlen), e0 = std::min<size_t>(x.target_end, tlen);
+            if (s0 < e0) windows.push_back({s0, e0});
+        }
+        const phr_alignment& p = res->aln[r.aln_off];
+        const std::string cig(res->cigar + p.cigar_off, p.cigar_len);
+        const double score = 1.0 - static_cast<double>(p.edit_distance) / static_cast<double>(std::max<size_t>(qlen, 1));
+        extract_variants(cig, p.target_start, q.data(), qlen, tg.bytes.data(), tlen, p.edit_distance, windows,
+                         tg.repeats, hs, he, nhs, score, radius, r.reverse, static_cast<uint32_t>(i), &out);
+    }
+    vout->read_variant_off[n] = out.v.size();
+    if (out.v.size() > vout->variant_capacity || out.cov.size() > vout->coverage_capacity ||
+        out.al.size() > vout->allele_capacity)
+        return PHR_ERR_CAPACITY;
+    if (!out.v.empty()) std::memcpy(vout->variants, out.v.data(), out.v.size() * sizeof(phr_variant));
+    if (!out.cov.empty()) std::memcpy(vout->coverage, out.cov.data(), out.cov.size() * 4);
+    if (!out.al.empty()) std::memcpy(vout->alleles, out.al.data(), out.al.size() * sizeof(phr_allele));
+    vout->variant_used = out.v.size();
+    vout->coverage_used = out.cov.size();
+    vout->allele_used = out.al.size();
     return PHR_OK;
 }
 

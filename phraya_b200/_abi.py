@@ -198,6 +198,31 @@ class AlignStats(C.Structure):
     ]
 
 
+class VariantConfig(C.Structure):
+    _fields_ = [
+        ("coverage_radius", C.c_uint32),
+        ("_pad", C.c_uint32),
+        ("hotspot_start", C.c_void_p),
+        ("hotspot_end", C.c_void_p),
+        ("n_hotspots", C.c_uint64),
+    ]
+
+
+class VariantArena(C.Structure):
+    _fields_ = [
+        ("read_variant_off", C.c_void_p),
+        ("variants", C.c_void_p),
+        ("variant_capacity", C.c_uint64),
+        ("variant_used", C.c_uint64),
+        ("coverage", C.c_void_p),
+        ("coverage_capacity", C.c_uint64),
+        ("coverage_used", C.c_uint64),
+        ("alleles", C.c_void_p),
+        ("allele_capacity", C.c_uint64),
+        ("allele_used", C.c_uint64),
+    ]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [
         ("align", AlignConfig),
@@ -259,6 +284,12 @@ PROTOTYPES = {
                                          C.POINTER(ChainArena)]),
     "phr_align_reads": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(ReadBatch), C.POINTER(AlignConfig),
                                     C.POINTER(ReadResultArena), C.POINTER(AlignStats)]),
+    "phr_align_reads_variants": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(ReadBatch),
+                                             C.POINTER(AlignConfig), C.POINTER(ReadResultArena),
+                                             C.POINTER(VariantConfig), C.POINTER(VariantArena),
+                                             C.POINTER(AlignStats)]),
+    "phr_index_repeat_regions": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                             C.POINTER(C.c_uint64)]),
     "phr_server_create": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(ServerConfig),
                                       C.POINTER(C.c_void_p)]),
     "phr_server_submit": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)]),

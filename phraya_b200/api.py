@@ -16,7 +16,7 @@ import threading
 import numpy as np
 
 from . import _abi as A
-from .batch import ALN_DTYPE, PackedPairs, PackedReads, READ_RESULT_DTYPE
+from .batch import ALLELE_DTYPE, ALN_DTYPE, PackedPairs, PackedReads, READ_RESULT_DTYPE, VARIANT_DTYPE
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libphraya_b200.so")
@@ -255,6 +255,16 @@ class Index:
                 "occurrence_cap": inf.occurrence_cap, "target_len": inf.target_len,
                 "device_bytes": inf.device_bytes}
 
+    def repeat_regions(self):
+        """TargetContext::repeat_regions: [(start, end_inclusive), ...] (phr_index_repeat_regions)."""
+        n = C.c_uint64(0)
+        self._eng.check(self._lib.phr_index_repeat_regions(self._h, None, None, 0, C.byref(n)))
+        st = np.zeros(max(n.value, 1), dtype=np.uint32)
+        en = np.zeros(max(n.value, 1), dtype=np.uint32)
+        self._eng.check(self._lib.phr_index_repeat_regions(self._h, st.ctypes.data, en.ctypes.data, n.value,
+                                                           C.byref(n)))
+        return [(int(a), int(b)) for a, b in zip(st[:n.value], en[:n.value])]
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.phr_index_destroy(self._h)
@@ -334,6 +344,67 @@ def _align_packed(engine, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AF
     return rr[:n], aln[:arena.aln_used], cig[:arena.cigar_used], st
 
 
+def _align_packed_variants(engine, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, radius=0,
+                           hotspots=()):
+    """phr_align_reads_variants; grows the variant arena once if the first guess is short.
+    -> (rr, aln, cig, stats, read_variant_off, variants, coverage, alleles)"""
+    n = packed.n
+    rr = np.zeros(max(n, 1), dtype=READ_RESULT_DTYPE)
+    K = 1 if strategy == A.FAST else 2 if strategy == A.BALANCED else 50
+    acap = 2 * K * n + 16
+    aln = np.empty(acap, dtype=ALN_DTYPE)
+    ccap = 2 * K * (6 * int(packed.len.astype(np.uint64).sum()) + 16 * n) + 64
+    cig = np.empty(ccap, dtype=np.uint8)
+    hs = np.ascontiguousarray([h[0] for h in hotspots], dtype=np.uint32)
+    he = np.ascontiguousarray([h[1] for h in hotspots], dtype=np.uint32)
+    vcfg = A.VariantConfig(radius, 0, hs.ctypes.data if len(hs) else None, he.ctypes.data if len(he) else None,
+                           len(hs))
+    r = radius or (150 if strategy == A.FAST else 50 if strategy == A.BALANCED else 25)
+    vcap = max(16, n * 8)
+    sizes = [vcap, vcap * (2 * r + 1), vcap * 2]
+    off = np.zeros(n + 1, dtype=np.uint64)
+    cfg = A.AlignConfig(strategy, gap_model)
+    b = packed.batch()
+    for _ in range(2):
+        var = np.empty(sizes[0], dtype=VARIANT_DTYPE)
+        cov = np.empty(sizes[1], dtype=np.uint32)
+        al = np.empty(sizes[2], dtype=ALLELE_DTYPE)
+        va = A.VariantArena(off.ctypes.data, var.ctypes.data, sizes[0], 0, cov.ctypes.data, sizes[1], 0,
+                            al.ctypes.data, sizes[2], 0)
+        arena = A.ReadResultArena(rr.ctypes.data, aln.ctypes.data, acap, 0, cig.ctypes.data, ccap, 0)
+        stats = A.AlignStats()
+        st = engine._lib.phr_align_reads_variants(engine.handle, index.handle, C.byref(b), C.byref(cfg),
+                                                  C.byref(arena), C.byref(vcfg), C.byref(va), C.byref(stats))
+        if st == A.PHR_ERR_CAPACITY and (va.variant_used > sizes[0] or va.coverage_used > sizes[1]
+                                         or va.allele_used > sizes[2]):
+            sizes = [max(sizes[0], int(va.variant_used)), max(sizes[1], int(va.coverage_used)),
+                     max(sizes[2], int(va.allele_used))]
+            continue
+        engine.check(st)
+        break
+    stt = (stats.placed, stats.no_seed, stats.below_threshold, stats.fast_cutoff, stats.no_alignment)
+    return (rr[:n], aln[:arena.aln_used], cig[:arena.cigar_used], stt, off, var[:va.variant_used],
+            cov[:va.coverage_used], al[:va.allele_used])
+
+
+def unpack_variants(off, var, cov, al):
+    """-> per read [(position, ref, type, in_repeat, strand, ed, confidence, kmer_uniqueness,
+    local_coverage, coverage_variant_offset, [(allele, count), ...]), ...]"""
+    out = []
+    for i in range(len(off) - 1):
+        rows = []
+        for v in var[int(off[i]):int(off[i + 1])]:
+            c0 = int(v["coverage_off"])
+            a0 = int(v["allele_off"])
+            rows.append((int(v["position"]), int(v["ref_base"]), int(v["variant_type"]), int(v["in_tandem_repeat"]),
+                         int(v["strand"]), int(v["edit_distance"]), float(v["confidence"]),
+                         float(v["kmer_uniqueness"]), cov[c0:c0 + int(v["coverage_len"])].tolist(),
+                         int(v["coverage_variant_offset"]),
+                         [(int(a["base"]), int(a["count"])) for a in al[a0:a0 + int(v["n_alleles"])]]))
+        out.append(rows)
+    return out
+
+
 def unpack_reads(rr, aln, cig):
     """-> [(outcome, has_result, reverse, [(cigar, ed, qs, qe, ts, te), ...])]"""
     out = []
@@ -359,7 +430,19 @@ def _engine_align_reads(self, index, reads, strategy=A.BALANCED, gap_model=A.GAP
     return unpack_reads(rr, aln, cig), st
 
 
+def _engine_align_reads_variants(self, index, reads, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, radius=0,
+                                 hotspots=(), stored=None):
+    """align_read with variant observations: -> (read results, stats, per-read variants)."""
+    packed = reads if isinstance(reads, PackedReads) else PackedReads(reads, stored)
+    rr, aln, cig, st, off, var, cov, al = _align_packed_variants(self, index, packed, strategy, gap_model, radius,
+                                                                 hotspots)
+    return unpack_reads(rr, aln, cig), st, unpack_variants(off, var, cov, al)
+
+
 Engine.index = _engine_index
+Engine.align_reads_variants = _engine_align_reads_variants
+Engine.align_packed_variants = lambda self, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, radius=0, \
+    hotspots=(): _align_packed_variants(self, index, packed, strategy, gap_model, radius, hotspots)
 Engine.align_reads = _engine_align_reads
 Engine.align_packed = lambda self, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE: _align_packed(
     self, index, packed, strategy, gap_model)

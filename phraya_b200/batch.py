@@ -66,6 +66,15 @@ class PackedPairs:
         return int(2 * (self.q_len.astype(np.uint64).sum() + self.t_len.astype(np.uint64).sum())) + 16
 
 
+VARIANT_DTYPE = np.dtype([("position", "<u4"), ("ref_base", "u1"), ("variant_type", "u1"),
+                          ("in_tandem_repeat", "u1"), ("strand", "u1"), ("read", "<u4"), ("edit_distance", "<u4"),
+                          ("confidence", "<f8"), ("kmer_uniqueness", "<f8"), ("coverage_off", "<u8"),
+                          ("coverage_len", "<u4"), ("coverage_variant_offset", "<u4"), ("allele_off", "<u8"),
+                          ("n_alleles", "<u4"), ("_pad", "<u4")])
+assert VARIANT_DTYPE.itemsize == 64
+
+ALLELE_DTYPE = np.dtype([("base", "u1"), ("_pad", "u1", (3,)), ("count", "<u4")])
+
 READ_RESULT_DTYPE = np.dtype([("outcome", "<i4"), ("has_result", "u1"), ("reverse", "u1"), ("_pad", "<u2"),
                               ("n_aln", "<u4"), ("_pad2", "<u4"), ("aln_off", "<u8")])
 

@@ -14,6 +14,8 @@
 // the SplitMix64 finalizer as order key, leftmost minimum per window, consecutive
 // duplicates emitted once; pairs are (key, k-mer start).
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 #include <cub/device/device_segmented_sort.cuh>
 
 #include <algorithm>
@@ -764,6 +766,223 @@ __global__ void pack_out_kernel(PackOutArgs P) {
 
 
 
+// ---------------------------------------------------------------------------
+// Tandem repeats (detect_tandem_repeats, phraya-core/src/lib.rs:79-135)
+// ---------------------------------------------------------------------------
+__device__ __host__ __forceinline__ uint8_t upper_ascii(uint8_t c) {
+    return (c >= 'a' && c <= 'z') ? static_cast<uint8_t>(c - 32) : c;
+}
+
+// The detector walks left to right; at a walk position p it takes the first period P in
+// 4, 3, 2 with p + 3P <= n whose unit occurs three times in a row, i.e. s[i] == s[i + P]
+// for every i in [p, p + 2P) (upper-cased bytes), and jumps past the repeat. Whether p
+// passes that test does not depend on the walk, so every position is tested here in
+// parallel; the walk itself then only visits the flagged positions (host, in order).
+__global__ void repeat_candidate_kernel(const uint8_t* s, uint64_t base, uint64_t cnt, uint64_t n, uint8_t* flag) {
+    const uint64_t j = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (j >= cnt) return;
+    const uint64_t p = base + j;
+    uint8_t f = 0;
+    if (p + 6 <= n) {
+        for (int P = 4; P >= 2 && !f; --P) {
+            if (p + 3 * static_cast<uint64_t>(P) > n) continue;
+            bool ok = true;
+            for (int i = 0; i < 2 * P && ok; ++i) ok = upper_ascii(s[p + i]) == upper_ascii(s[p + i + P]);
+            if (ok) f = static_cast<uint8_t>(P);
+        }
+    }
+    flag[j] = f;
+}
+
+// ---------------------------------------------------------------------------
+// Variant observations (extract_variants_from_cigar, phraya-align/src/executor.rs:814-1046)
+// ---------------------------------------------------------------------------
+struct VariantArgs {
+    uint64_t n;
+    const phr_read_result* res;     // packed results: read r's alignments at aln[aln_off ..], primary first
+    const phr_alignment* aln;
+    const char* cigar;
+    const uint8_t* qarena;          // read r forward at rd_off[r], reverse complement at rd_off[n + r]
+    const uint64_t* rd_off;
+    const uint32_t* rd_len;
+    const uint8_t* target;
+    uint64_t tlen;
+    const uint32_t* rep_start;      // tandem-repeat regions, sorted, end inclusive
+    const uint32_t* rep_end;
+    uint64_t n_rep;
+    const uint32_t* hs_start;       // hotspot intervals [start, end), sorted
+    const uint32_t* hs_end;
+    uint64_t n_hs;
+    uint64_t radius;
+    uint64_t* cnt;                  // count pass: per read variants [r], coverage cells [n+1+r], alleles [2(n+1)+r]
+    const uint64_t* off;            // write pass: exclusive scans of cnt, same layout
+    phr_variant* var;
+    uint32_t* cov;
+    phr_allele* al;
+};
+
+// partition_point(start <= pos) over a sorted array: the number of entries <= pos.
+__device__ __forceinline__ uint64_t upper_bound_u32(const uint32_t* a, uint64_t n, uint64_t pos) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= pos) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One warp per read. Every lane parses the primary CIGAR (the same bytes, so the loads
+// broadcast and control flow stays warp-uniform); the lanes split each variant's
+// coverage cells and the insertion allele counts. WRITE = false counts the read's
+// outputs, WRITE = true writes them at the scanned offsets.
+template <bool WRITE>
+__global__ void variant_kernel(VariantArgs V) {
+    const uint64_t r = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= V.n) return;
+    const uint64_t n1 = V.n + 1;
+    uint64_t nv = 0, nc = 0, na = 0;
+    if (WRITE) {
+        nv = V.off[r];
+        nc = V.off[n1 + r];
+        na = V.off[2 * n1 + r];
+    }
+    const phr_read_result rr = V.res[r];
+    if (rr.has_result && rr.n_aln) {
+        const phr_alignment pa = V.aln[rr.aln_off];
+        const uint8_t* q = V.qarena + V.rd_off[rr.reverse ? V.n + r : r];
+        const uint64_t qlen = V.rd_len[r];
+        const uint64_t tlen = V.tlen;
+        // primary_score (executor.rs:713) times kmer_uniqueness is the confidence.
+        const double score =
+            1.0 - static_cast<double>(pa.edit_distance) / static_cast<double>(qlen > 1 ? qlen : 1);
+        const char* c = V.cigar + pa.cigar_off;
+        const uint32_t clen = pa.cigar_len;
+        auto emit = [&](uint64_t tp, uint8_t ref, uint8_t type, uint64_t ins_lo, uint64_t ins_hi, uint8_t allele) {
+            const uint64_t ws = tp >= V.radius ? tp - V.radius : 0;
+            const uint64_t we = min(tp + V.radius + 1, tlen);
+            const uint64_t cl = we - ws;
+            // alleles: one for a SNP / deletion, the distinct inserted bytes for an insertion
+            uint32_t bm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            uint32_t nal = 1;
+            if (type == 1) {
+                for (uint64_t k = ins_lo + lane; k < ins_hi; k += 32) {
+                    const uint32_t b = q[k];
+#pragma unroll
+                    for (int w = 0; w < 8; ++w)
+                        if ((b >> 5) == static_cast<uint32_t>(w)) bm[w] |= 1u << (b & 31);
+                }
+                nal = 0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) {
+                    bm[w] = __reduce_or_sync(0xffffffffu, bm[w]);
+                    nal += __popc(bm[w]);
+                }
+            }
+            if (WRITE) {
+                for (uint64_t j = lane; j < cl; j += 32) {  // get_abs_multi over the read's windows
+                    const uint64_t pos = ws + j;
+                    uint32_t cv = 0;
+                    for (uint32_t a = 0; a < rr.n_aln; ++a) {
+                        const phr_alignment& x = V.aln[rr.aln_off + a];
+                        const uint64_t s0 = min(static_cast<uint64_t>(x.target_start), tlen);
+                        const uint64_t e0 = min(static_cast<uint64_t>(x.target_end), tlen);
+                        cv += (pos >= s0 && pos < e0) ? 1u : 0u;
+                    }
+                    V.cov[nc + j] = cv;
+                }
+                if (type == 1) {
+                    uint32_t k_out = 0;
+#pragma unroll
+                    for (int w = 0; w < 8; ++w) {
+                        uint32_t bits = bm[w];
+                        while (bits) {
+                            const uint32_t b = static_cast<uint32_t>(w) * 32 + (__ffs(bits) - 1);
+                            bits &= bits - 1;
+                            uint32_t cntb = 0;
+                            for (uint64_t k = ins_lo + lane; k < ins_hi; k += 32) cntb += q[k] == b ? 1u : 0u;
+                            cntb = __reduce_add_sync(0xffffffffu, cntb);
+                            if (lane == 0) {
+                                phr_allele o;
+                                o.base = static_cast<uint8_t>(b);
+                                o._pad[0] = o._pad[1] = o._pad[2] = 0;
+                                o.count = cntb;
+                                V.al[na + k_out] = o;
+                            }
+                            ++k_out;
+                        }
+                    }
+                } else if (lane == 0) {
+                    phr_allele o;
+                    o.base = allele;
+                    o._pad[0] = o._pad[1] = o._pad[2] = 0;
+                    o.count = 1;
+                    V.al[na] = o;
+                }
+                if (lane == 0) {
+                    phr_variant v;
+                    v.position = static_cast<uint32_t>(tp);
+                    v.ref_base = ref;
+                    v.variant_type = type;
+                    const uint64_t ri = upper_bound_u32(V.rep_start, V.n_rep, tp);
+                    v.in_tandem_repeat = (ri > 0 && tp < V.rep_end[ri - 1]) ? 1 : 0;
+                    v.strand = rr.reverse;
+                    v.read = static_cast<uint32_t>(r);
+                    v.edit_distance = pa.edit_distance;
+                    const uint64_t hi = upper_bound_u32(V.hs_start, V.n_hs, static_cast<uint32_t>(tp));
+                    v.kmer_uniqueness = (hi > 0 && static_cast<uint32_t>(tp) < V.hs_end[hi - 1]) ? 0.0 : 1.0;
+                    v.confidence = v.kmer_uniqueness * score;
+                    v.coverage_off = nc;
+                    v.coverage_len = static_cast<uint32_t>(cl);
+                    v.coverage_variant_offset = static_cast<uint32_t>(tp - ws);
+                    v.allele_off = na;
+                    v.n_alleles = nal;
+                    v._pad = 0;
+                    V.var[nv] = v;
+                }
+            }
+            nv += 1;
+            nc += cl;
+            na += nal;
+        };
+        uint64_t qp = 0, tp = pa.target_start;
+        uint32_t i = 0;
+        while (i < clen) {
+            uint64_t count = 0;
+            bool digits = false;
+            while (i < clen && c[i] >= '0' && c[i] <= '9') {
+                count = count * 10 + static_cast<uint64_t>(c[i] - '0');
+                ++i;
+                digits = true;
+            }
+            if (i >= clen) break;
+            const char op = c[i++];
+            if (!digits) count = 1;  // parse_cigar: an empty count reads as 1
+            if (op == 'M') {
+                qp += count;
+                tp += count;
+            } else if (op == 'X') {
+                for (uint64_t k = 0; k < count; ++k)
+                    if (qp + k < qlen && tp + k < tlen) emit(tp + k, V.target[tp + k], 0, 0, 0, q[qp + k]);
+                qp += count;
+                tp += count;
+            } else if (op == 'I') {  // target bases absent from the read: a deletion at tp
+                if (tp < tlen && qp < qlen) emit(tp, V.target[tp], 2, 0, 0, '.');
+                tp += count;
+            } else if (op == 'D') {  // read bases absent from the target: an insertion at tp
+                if (qp < qlen && tp < tlen) emit(tp, '.', 1, qp, min(qp + count, qlen), 0);
+                qp += count;
+            }
+        }
+    }
+    if (!WRITE && lane == 0) {
+        V.cnt[r] = nv;
+        V.cnt[n1 + r] = nc;
+        V.cnt[2 * n1 + r] = na;
+    }
+}
+
 __global__ void offset_add_kernel(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t add) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i < n) out[i] = in[i] + add;
@@ -949,6 +1168,79 @@ static phr_status build_index_from_sketch(Ctx* ctx, phr_index* idx, const uint64
     return PHR_OK;
 }
 
+// detect_tandem_repeats (phraya-core/src/lib.rs:79-135, min_repeat_count 3) over the
+// index's target: the device flags every position that passes the walk's test, the host
+// walks the flagged positions in order (skipping those inside an accepted repeat) and
+// extends each accepted repeat unit by unit. `target` is the caller's host copy.
+static phr_status detect_repeats(Ctx* ctx, phr_index* idx, const uint8_t* target) {
+    const uint64_t n = idx->target_len;
+    idx->rep_start.clear();
+    idx->rep_end.clear();
+    cudaStream_t st = ctx->stream;
+    if (n >= 6) {
+        const uint64_t chunk = std::min<uint64_t>(n, 1ull << 28);
+        DeviceArena& A = ctx->pipe;
+        A.reset();
+        size_t tb = 0;
+        cub::CountingInputIterator<uint32_t> it(0);
+        cub::DeviceSelect::Flagged(nullptr, tb, it, static_cast<const uint8_t*>(nullptr),
+                                   static_cast<uint32_t*>(nullptr), static_cast<int*>(nullptr),
+                                   static_cast<int>(chunk), st);
+        PHR_CUDA_TRY(ctx, A.reserve(chunk * 5 + tb + (4 << 20)));
+        uint8_t* flag = static_cast<uint8_t*>(A.take(chunk + 64));
+        uint32_t* cand = static_cast<uint32_t*>(A.take(chunk * 4 + 64));
+        int* d_cnt = static_cast<int*>(A.take(64));
+        void* tmp = A.take(tb + 256);
+        if (!tmp) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (repeat scan)");
+        std::vector<uint32_t> h;
+        uint64_t cur = 0;
+        for (uint64_t base = 0; base < n; base += chunk) {
+            const uint64_t cnt = std::min<uint64_t>(chunk, n - base);
+            {
+                KernelScope ks(ctx, "repeat_candidates");
+                repeat_candidate_kernel<<<blocks_for(cnt, 256), 256, 0, st>>>(idx->d_target, base, cnt, n, flag);
+            }
+            size_t t2 = tb;
+            cub::DeviceSelect::Flagged(tmp, t2, cub::CountingInputIterator<uint32_t>(static_cast<uint32_t>(base)),
+                                       flag, cand, d_cnt, static_cast<int>(cnt), st);
+            int hc = 0;
+            PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&hc, d_cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+            h.resize(static_cast<size_t>(hc));
+            if (hc) PHR_CUDA_TRY(ctx, cudaMemcpy(h.data(), cand, static_cast<size_t>(hc) * 4, cudaMemcpyDeviceToHost));
+            for (uint32_t p : h) {
+                if (p < cur) continue;
+                int P = 4;
+                for (; P >= 2; --P) {  // the same test the device applied; the first period wins
+                    if (p + 3ull * P > n) continue;
+                    bool ok = true;
+                    for (int i = 0; i < 2 * P && ok; ++i) ok = upper_ascii(target[p + i]) == upper_ascii(target[p + i + P]);
+                    if (ok) break;
+                }
+                if (P < 2) continue;
+                uint64_t end = p + static_cast<uint64_t>(P);
+                while (end + P <= n) {
+                    bool eq = true;
+                    for (int i = 0; i < P && eq; ++i) eq = upper_ascii(target[p + i]) == upper_ascii(target[end + i]);
+                    if (!eq) break;
+                    end += P;
+                }
+                idx->rep_start.push_back(p);
+                idx->rep_end.push_back(static_cast<uint32_t>(end - 1));
+                cur = end;
+            }
+        }
+    }
+    const uint64_t nr = idx->rep_start.size();
+    if (nr) {
+        PHR_CUDA_TRY(ctx, cudaMalloc(&idx->d_rep, nr * 8));
+        PHR_CUDA_TRY(ctx, cudaMemcpy(idx->d_rep, idx->rep_start.data(), nr * 4, cudaMemcpyHostToDevice));
+        PHR_CUDA_TRY(ctx, cudaMemcpy(idx->d_rep + nr, idx->rep_end.data(), nr * 4, cudaMemcpyHostToDevice));
+        idx->device_bytes += nr * 8;
+    }
+    return PHR_OK;
+}
+
 phr_status index_create(Ctx* ctx, const uint8_t* target, uint64_t tlen, const phr_sketch* sketch, int alphabet,
                         phr_index** out) {
     init_penalty_table(ctx->device);
@@ -1018,6 +1310,7 @@ phr_status index_create(Ctx* ctx, const uint8_t* target, uint64_t tlen, const ph
         }
     }
     phr_status s = build_index_from_sketch(ctx, idx, hv.data(), hp.data(), hv.size());
+    if (s == PHR_OK) s = detect_repeats(ctx, idx, target);
     if (s != PHR_OK) {
         delete idx;
         return s;
@@ -1173,6 +1466,9 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rd_len, d_len, n * 4, cudaMemcpyDeviceToDevice, st));
     PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rd_len + n, d_len, n * 4, cudaMemcpyDeviceToDevice, st));
     uint64_t* rc_off = rd_off + n;
+    out->qarena = qarena;
+    out->rd_off = rd_off;
+    out->rd_len = rd_len;
     if (n) {
         KernelScope ks(ctx, "rc_offsets");
         offset_add_kernel<<<blocks_for(n, T), T, 0, st>>>(d_off, rc_off, n, seq_bytes);
@@ -1398,7 +1694,7 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
 // Packs device results into caller-visible device buffers, then copies them to the host
 // arena. Returns PHR_ERR_CAPACITY if the host arena is too small.
 static phr_status pack_to_host(Ctx* ctx, DeviceArena& A, uint64_t n, const AlignOutput& o,
-                               phr_read_result_arena* host, phr_align_stats* stats) {
+                               phr_read_result_arena* host, phr_align_stats* stats, PackedDev* dev = nullptr) {
     cudaStream_t st = ctx->stream;
     const unsigned T = 256;
     uint64_t* n_aln = static_cast<uint64_t*>(A.take((n + 1) * 8 + 8));
@@ -1446,6 +1742,11 @@ static phr_status pack_to_host(Ctx* ctx, DeviceArena& A, uint64_t n, const Align
     PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     host->aln_used = tot[0];
     host->cigar_used = tot[1];
+    if (dev) {
+        dev->res = d_res;
+        dev->aln = d_aln;
+        dev->cigar = d_cig;
+    }
     if (stats) {
         stats->placed += hst[PHR_OUT_PLACED];
         stats->no_seed += hst[PHR_OUT_NO_SEED];
@@ -1456,8 +1757,91 @@ static phr_status pack_to_host(Ctx* ctx, DeviceArena& A, uint64_t n, const Align
     return PHR_OK;
 }
 
+// Variant observations of the packed results (align_read, executor.rs:735-775): a count
+// pass, three exclusive scans, a write pass into device buffers, then one copy per array
+// into the caller's arena. On PHR_ERR_CAPACITY the arena's *_used fields hold the sizes
+// needed.
+static phr_status variants_to_host(Ctx* ctx, DeviceArena& A, uint64_t n, const phr_index* idx, const AlignOutput& o,
+                                   const PackedDev& pd, const phr_align_config& cfg, const phr_variant_config* vcfg,
+                                   phr_variant_arena* vout) {
+    cudaStream_t st = ctx->stream;
+    const unsigned T = 256;
+    VariantArgs V{};
+    V.n = n;
+    V.res = pd.res;
+    V.aln = pd.aln;
+    V.cigar = pd.cigar;
+    V.qarena = o.qarena;
+    V.rd_off = o.rd_off;
+    V.rd_len = o.rd_len;
+    V.target = idx->d_target;
+    V.tlen = idx->target_len;
+    V.n_rep = idx->rep_start.size();
+    V.rep_start = idx->d_rep;
+    V.rep_end = idx->d_rep ? idx->d_rep + V.n_rep : nullptr;
+    // AlignConfig::new (executor.rs:124-128): the strategy's coverage radius
+    V.radius = vcfg && vcfg->coverage_radius ? vcfg->coverage_radius
+               : cfg.strategy == PHR_FAST    ? 150
+               : cfg.strategy == PHR_BALANCED ? 50
+                                              : 25;
+    const uint64_t nhs = vcfg && vcfg->hotspot_start && vcfg->hotspot_end ? vcfg->n_hotspots : 0;
+    V.n_hs = nhs;
+    if (nhs) {
+        uint32_t* hs = static_cast<uint32_t*>(A.take(nhs * 8 + 16));
+        if (!hs) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (hotspots)");
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(hs, vcfg->hotspot_start, nhs * 4, cudaMemcpyHostToDevice, st));
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(hs + nhs, vcfg->hotspot_end, nhs * 4, cudaMemcpyHostToDevice, st));
+        V.hs_start = hs;
+        V.hs_end = hs + nhs;
+    }
+    const uint64_t n1 = n + 1;
+    uint64_t* cnt = static_cast<uint64_t*>(A.take(3 * n1 * 8 + 8));
+    uint64_t* off = static_cast<uint64_t*>(A.take(3 * n1 * 8 + 8));
+    if (!off) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (variant counts)");
+    for (int k = 0; k < 3; ++k) PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + k * n1 + n, 0, 8, st));
+    V.cnt = cnt;
+    if (n) {
+        KernelScope ks(ctx, "variant_count");
+        variant_kernel<false><<<blocks_for(n * 32, T), T, 0, st>>>(V);
+    }
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, static_cast<int>(n1), st);
+    void* tmp = A.take(tb + 256);
+    if (!tmp) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (variant scan)");
+    for (int k = 0; k < 3; ++k) {
+        size_t t2 = tb;
+        cub::DeviceScan::ExclusiveSum(tmp, t2, cnt + k * n1, off + k * n1, static_cast<int>(n1), st);
+    }
+    uint64_t tot[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&tot[k], off + k * n1 + n, 8, cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    vout->variant_used = tot[0];
+    vout->coverage_used = tot[1];
+    vout->allele_used = tot[2];
+    if (tot[0] > vout->variant_capacity) return set_error(ctx, PHR_ERR_CAPACITY, "variant arena too small");
+    if (tot[1] > vout->coverage_capacity) return set_error(ctx, PHR_ERR_CAPACITY, "coverage arena too small");
+    if (tot[2] > vout->allele_capacity) return set_error(ctx, PHR_ERR_CAPACITY, "allele arena too small");
+    V.off = off;
+    V.var = static_cast<phr_variant*>(A.take(tot[0] * sizeof(phr_variant) + 8));
+    V.cov = static_cast<uint32_t*>(A.take(tot[1] * 4 + 8));
+    V.al = static_cast<phr_allele*>(A.take(tot[2] * sizeof(phr_allele) + 8));
+    if (!V.al) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (variant outputs)");
+    if (n) {
+        KernelScope ks(ctx, "variant_write");
+        variant_kernel<true><<<blocks_for(n * 32, T), T, 0, st>>>(V);
+    }
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(vout->read_variant_off, off, n1 * 8, cudaMemcpyDeviceToHost, st));
+    if (tot[0]) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(vout->variants, V.var, tot[0] * sizeof(phr_variant), cudaMemcpyDeviceToHost, st));
+    if (tot[1]) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(vout->coverage, V.cov, tot[1] * 4, cudaMemcpyDeviceToHost, st));
+    if (tot[2]) PHR_CUDA_TRY(ctx, cudaMemcpyAsync(vout->alleles, V.al, tot[2] * sizeof(phr_allele), cudaMemcpyDeviceToHost, st));
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return PHR_OK;
+}
+
 phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch* rb, const phr_align_config& cfg,
-                            phr_read_result_arena* out, phr_align_stats* stats) {
+                            phr_read_result_arena* out, phr_align_stats* stats, const phr_variant_config* vcfg,
+                            phr_variant_arena* vout) {
     cudaStream_t st = ctx->stream;
     const uint64_t n = rb->n_reads;
     out->aln_used = 0;
@@ -1500,6 +1884,7 @@ phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch
         }
     }
     AlignOutput o;
+    PackedDev pd;
     phr_status s;
     {
         HostScope hs(ctx, "host:device_pipeline");
@@ -1508,7 +1893,11 @@ phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch
     if (s != PHR_OK) return s;
     {
         HostScope hs(ctx, "host:pack_to_host");
-        s = pack_to_host(ctx, A, n, o, out, stats);
+        s = pack_to_host(ctx, A, n, o, out, stats, vout ? &pd : nullptr);
+    }
+    if (s == PHR_OK && vout) {
+        HostScope hs(ctx, "host:variants");
+        s = variants_to_host(ctx, A, n, idx, o, pd, cfg, vcfg, vout);
     }
     if (ctx->timing) ctx->resolve_timings();
     return s;
@@ -1517,6 +1906,7 @@ phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch
 }  // namespace phr
 
 phr_index::~phr_index() {
+    if (d_rep) cudaFree(d_rep);
     if (d_block) cudaFree(d_block);
     if (d_target) cudaFree(d_target);
 }
@@ -1690,7 +2080,40 @@ phr_status phr_align_reads(phr_ctx* c, const phr_index* idx, const phr_read_batc
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
     if (cfg->strategy < PHR_FAST || cfg->strategy > PHR_SENSITIVE) return phr::set_error(ctx, PHR_ERR_ARG, "strategy");
-    return phr::align_reads_host(ctx, idx, reads, *cfg, out, stats);
+    return phr::align_reads_host(ctx, idx, reads, *cfg, out, stats, nullptr, nullptr);
+}
+
+phr_status phr_align_reads_variants(phr_ctx* c, const phr_index* idx, const phr_read_batch* reads,
+                                    const phr_align_config* cfg, phr_read_result_arena* out,
+                                    const phr_variant_config* vcfg, phr_variant_arena* vout,
+                                    phr_align_stats* stats) {
+    if (!c || !idx || !reads || !cfg || !out || !vout || !vout->read_variant_off ||
+        (reads->n_reads && (!reads->off || !reads->len || !out->reads)))
+        return PHR_ERR_ARG;
+    if (vcfg && vcfg->n_hotspots && (!vcfg->hotspot_start || !vcfg->hotspot_end)) return PHR_ERR_ARG;
+    phr::Ctx* ctx = &c->impl;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (cfg->strategy < PHR_FAST || cfg->strategy > PHR_SENSITIVE) return phr::set_error(ctx, PHR_ERR_ARG, "strategy");
+    vout->variant_used = vout->coverage_used = vout->allele_used = 0;
+    if (reads->n_reads == 0) {
+        vout->read_variant_off[0] = 0;
+        out->aln_used = out->cigar_used = 0;
+        return PHR_OK;
+    }
+    return phr::align_reads_host(ctx, idx, reads, *cfg, out, stats, vcfg, vout);
+}
+
+phr_status phr_index_repeat_regions(const phr_index* idx, uint32_t* start, uint32_t* end, uint64_t cap, uint64_t* n) {
+    if (!idx || !n || (cap && (!start || !end))) return PHR_ERR_ARG;
+    const uint64_t nr = idx->rep_start.size();
+    const uint64_t k = std::min(nr, cap);
+    if (k) {
+        std::memcpy(start, idx->rep_start.data(), k * 4);
+        std::memcpy(end, idx->rep_end.data(), k * 4);
+    }
+    *n = nr;
+    return PHR_OK;
 }
 
 }  // extern "C"

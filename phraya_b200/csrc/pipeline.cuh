@@ -1,6 +1,8 @@
 // pipeline.cuh -- device structures of the align_read pipeline (pipeline.cu).
 #pragma once
 
+#include <vector>
+
 #include "engine.cuh"
 
 namespace phr {
@@ -46,6 +48,16 @@ struct AlignOutput {
     char* eng_cigar[3] = {nullptr, nullptr, nullptr};
     uint64_t eng_pairs[3] = {0, 0, 0};
     uint64_t* stats = nullptr;             // 5 outcome counters
+    const uint8_t* qarena = nullptr;       // read r forward at rd_off[r], reverse complement at rd_off[n + r]
+    const uint64_t* rd_off = nullptr;
+    const uint32_t* rd_len = nullptr;
+};
+
+// Caller-layout results on the device (phr_read_result_arena order), kept by pack_to_host.
+struct PackedDev {
+    const phr_read_result* res = nullptr;
+    const phr_alignment* aln = nullptr;
+    const char* cigar = nullptr;
 };
 
 }  // namespace phr
@@ -58,6 +70,10 @@ struct phr_index {
     uint64_t n_min = 0, n_distinct = 0, device_bytes = 0;
     int alphabet = 0, k = 21, w = 11;
     void* d_block = nullptr;
+    // Tandem-repeat regions of the target (TargetContext::repeat_regions), sorted and
+    // non-overlapping, [start, end] with end inclusive; d_rep = starts then ends.
+    std::vector<uint32_t> rep_start, rep_end;
+    uint32_t* d_rep = nullptr;
     ~phr_index();
 };
 
@@ -79,6 +95,12 @@ phr_status align_reads_device(Ctx* ctx, const phr_index* idx, const uint8_t* d_s
                               const uint32_t* d_len, uint64_t n, uint64_t seq_bytes, const uint8_t* d_has_stored,
                               const uint64_t* d_s_off, const uint32_t* d_s_n, const uint64_t* d_s_val,
                               const uint32_t* d_s_pos, const phr_align_config& cfg, AlignOutput* out);
+
+// Host batch: upload, align_reads_device, pack into the caller's arena and, when `vout`
+// is given, the variant observations of every read with a result.
+phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch* rb, const phr_align_config& cfg,
+                            phr_read_result_arena* out, phr_align_stats* stats,
+                            const phr_variant_config* vcfg = nullptr, phr_variant_arena* vout = nullptr);
 
 size_t align_arena_need(uint64_t n_reads, uint64_t seq_bytes, uint64_t stored_total);
 

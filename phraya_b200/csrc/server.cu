@@ -27,10 +27,6 @@
 
 #include "pipeline.cuh"
 
-namespace phr {
-phr_status align_reads_host(Ctx* ctx, const phr_index* idx, const phr_read_batch* rb, const phr_align_config& cfg,
-                            phr_read_result_arena* out, phr_align_stats* stats);
-}
 
 namespace {
 
