@@ -418,6 +418,32 @@ def run_pipeline(eng, dev, args):
         dt = time.perf_counter() - t0
         out[f"batched_{name}_reads_per_s"] = len(reads) / dt
         out[f"batched_{name}_placed_frac"] = st[0] / len(reads)
+    # variant observations of every read with a result (extract_variants_from_cigar with
+    # local coverage, executor.rs:735-775, 814-1096) on the device, in the same call
+    eng.align_packed_variants(idx, packed, A.BALANCED, A.GAP_AFFINE)  # warm-up
+    t0 = time.perf_counter()
+    vres = eng.align_packed_variants(idx, packed, A.BALANCED, A.GAP_AFFINE)
+    dt = time.perf_counter() - t0
+    n_var = len(vres[5])
+    out["batched_balanced_with_variants_reads_per_s"] = len(reads) / dt
+    out["variant_observations"] = n_var
+    out["coverage_cells"] = len(vres[6])
+    eng._lib.phr_ctx_reset_timing(eng.handle)
+    eng.set_timing(True)
+    eng.align_packed_variants(idx, packed, A.BALANCED, A.GAP_AFFINE)
+    kt = eng.kernel_times()
+    eng.set_timing(False)
+    vk_ms = sum(kt.get(k, (0, 0.0))[1] for k in ("variant_count", "variant_write"))
+    out["variant_kernels_ms"] = vk_ms
+    out["variant_observations_per_s_device"] = n_var / (vk_ms / 1000.0) if vk_ms > 0 else None
+    if not args.no_cpu:
+        import oracle as O
+        otg = O.Target(ref)
+        t0 = time.perf_counter()
+        O_res = otg.variants_packed(packed, vres[0], vres[1], vres[2], A.BALANCED)
+        cdt = time.perf_counter() - t0
+        out["variants_cpu_baseline"] = {"value": len(O_res[1]) / cdt, "unit": "observations/s", "cores": 1,
+                                        "kind": "port", "sample": f"{len(reads)} reads, balanced, 1 Mbp"}
     # one read per call (the reference API's shape), on a sample
     k = min(300, len(reads))
     one = [PackedReads([r]) for r in reads[:k]]

@@ -500,6 +500,27 @@ phr_status phr_align_reads_variants(phr_ctx* ctx, const phr_index* idx, const ph
 phr_status phr_index_repeat_regions(const phr_index* idx, uint32_t* start, uint32_t* end, uint64_t cap,
                                     uint64_t* n);
 
+/*
+ * Genome coverage track, resident on the device, merged batch by batch as the CLI's
+ * merge_result does (phraya-cli/src/main.rs:556-572): every alignment of a read with a
+ * result contributes its window [min(target_start, len), min(target_end, len)) with
+ * per-position count 1, quantized per window by quantize_coverage
+ * (executor.rs:1092-1096, ((c + 2) / 5) * 5) before it is added.
+ * PHR_COVERAGE_QUANTIZED reproduces that track exactly (quantize(1) = 0, so it stays
+ * all zero, as the reference's does); PHR_COVERAGE_DEPTH adds the raw count instead
+ * (read depth). Tracks are target_len uint32 entries.
+ */
+typedef struct phr_coverage phr_coverage;
+typedef enum { PHR_COVERAGE_QUANTIZED = 0, PHR_COVERAGE_DEPTH = 1 } phr_coverage_mode;
+
+phr_status phr_coverage_create(phr_ctx* ctx, const phr_index* idx, phr_coverage_mode mode, phr_coverage** out);
+/* Adds the windows of aln[0 .. n_aln) (host array; e.g. a phr_read_result_arena's
+ * aln[0 .. aln_used), which holds only alignments of reads with a result). */
+phr_status phr_coverage_add(phr_coverage* cov, const phr_alignment* aln, uint64_t n_aln);
+/* Copies the track out (len must equal the index's target_len). */
+phr_status phr_coverage_read(phr_coverage* cov, uint32_t* track, uint64_t len);
+void phr_coverage_destroy(phr_coverage* cov);
+
 /* ------------------------------------------------------------------------- */
 /* Serving loop: device-resident index, admission by free HBM, continuous    */
 /* batching. No counterpart in the reference (its CLI is batch-only).         */

@@ -71,6 +71,8 @@ def lib():
         L.orc_variants.argtypes = [C.c_void_p, C.POINTER(A.ReadBatch), C.POINTER(A.ReadResultArena),
                                    C.POINTER(A.AlignConfig), C.POINTER(A.VariantConfig),
                                    C.POINTER(A.VariantArena)]
+        L.orc_coverage_merge.restype = None
+        L.orc_coverage_merge.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int32, C.c_void_p]
         _lib = L
     return _lib
 
@@ -215,6 +217,15 @@ def tandem_repeats(seq):
     n = int(lib().orc_tandem_repeats(seq, len(seq), st.ctypes.data, en.ctypes.data, cap))
     assert n <= cap
     return [(int(a), int(b)) for a, b in zip(st[:n], en[:n])]
+
+
+def coverage_merge(aln, tlen, depth=False, track=None):
+    """merge_result's coverage accumulation over an ALN_DTYPE array; returns the track."""
+    if track is None:
+        track = np.zeros(tlen, dtype=np.uint32)
+    aln = np.ascontiguousarray(aln, dtype=ALN_DTYPE)
+    lib().orc_coverage_merge(aln.ctypes.data if len(aln) else None, len(aln), tlen, int(depth), track.ctypes.data)
+    return track
 
 
 def variant_config(radius=0, hotspots=()):

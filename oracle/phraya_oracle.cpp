@@ -1680,4 +1680,19 @@ int32_t orc_variants(void* tgt, const phr_read_batch* reads, const phr_read_resu
     return PHR_OK;
 }
 
+// Coverage merge of merge_result (phraya-cli/src/main.rs:556-572) over alignment windows
+// (compute_windowed_coverage, executor.rs:1071-1090: count 1 over [min(ts, len),
+// min(te, len))), each window quantized by quantize_coverage (executor.rs:1092-1096)
+// unless `depth`. Accumulates into track[0 .. tlen).
+void orc_coverage_merge(const phr_alignment* aln, uint64_t n, uint64_t tlen, int32_t depth, uint32_t* track) {
+    for (uint64_t a = 0; a < n; ++a) {
+        const uint64_t s0 = std::min<uint64_t>(aln[a].target_start, tlen);
+        const uint64_t e0 = std::min<uint64_t>(aln[a].target_end, tlen);
+        for (uint64_t p = s0; p < e0; ++p) {
+            const uint32_t c = 1;
+            track[p] += depth ? c : ((c + 2) / 5) * 5;
+        }
+    }
+}
+
 }  // extern "C"

@@ -23,6 +23,9 @@ ENGINE_MYERS_GLOBAL = 3
 ALPHABET_DNA = 0
 ALPHABET_PROTEIN = 1
 
+COVERAGE_QUANTIZED = 0
+COVERAGE_DEPTH = 1
+
 FAST = 0
 BALANCED = 1
 SENSITIVE = 2
@@ -290,6 +293,10 @@ PROTOTYPES = {
                                              C.POINTER(AlignStats)]),
     "phr_index_repeat_regions": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                                              C.POINTER(C.c_uint64)]),
+    "phr_coverage_create": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "phr_coverage_add": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "phr_coverage_read": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "phr_coverage_destroy": (None, [C.c_void_p]),
     "phr_server_create": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(ServerConfig),
                                       C.POINTER(C.c_void_p)]),
     "phr_server_submit": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64)]),

@@ -420,6 +420,36 @@ def unpack_reads(rr, aln, cig):
     return out
 
 
+class CoverageTrack:
+    """Device-resident genome coverage track merged batch by batch (phr_coverage_*)."""
+
+    def __init__(self, engine, index, mode=A.COVERAGE_QUANTIZED):
+        self._eng = engine
+        self._lib = engine._lib
+        self.len = int(index.info()["target_len"])
+        h = C.c_void_p()
+        engine.check(self._lib.phr_coverage_create(engine.handle, index.handle, mode, C.byref(h)))
+        self._h = h
+
+    def add(self, aln):
+        """Adds the windows of an alignment array (ALN_DTYPE), e.g. align_packed's `aln`."""
+        aln = np.ascontiguousarray(aln, dtype=ALN_DTYPE)
+        self._eng.check(self._lib.phr_coverage_add(self._h, aln.ctypes.data if len(aln) else None, len(aln)))
+
+    def read(self):
+        out = np.zeros(self.len, dtype=np.uint32)
+        self._eng.check(self._lib.phr_coverage_read(self._h, out.ctypes.data if self.len else None, self.len))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.phr_coverage_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 def _engine_index(self, target, alphabet=A.ALPHABET_DNA, sketch=None):
     return Index(self, target, alphabet, sketch)
 
@@ -440,6 +470,7 @@ def _engine_align_reads_variants(self, index, reads, strategy=A.BALANCED, gap_mo
 
 
 Engine.index = _engine_index
+Engine.coverage_track = lambda self, index, mode=A.COVERAGE_QUANTIZED: CoverageTrack(self, index, mode)
 Engine.align_reads_variants = _engine_align_reads_variants
 Engine.align_packed_variants = lambda self, index, packed, strategy=A.BALANCED, gap_model=A.GAP_AFFINE, radius=0, \
     hotspots=(): _align_packed_variants(self, index, packed, strategy, gap_model, radius, hotspots)

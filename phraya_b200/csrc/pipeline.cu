@@ -983,6 +983,23 @@ __global__ void variant_kernel(VariantArgs V) {
     }
 }
 
+// Coverage merge (phraya-cli/src/main.rs:556-572): one warp per alignment adds its
+// window's quantized count to the resident track. The window count is 1 everywhere
+// (compute_windowed_coverage, executor.rs:1071-1090), quantized per window
+// (quantize_coverage, executor.rs:1092-1096) unless `depth` asks for the raw count.
+__global__ void coverage_add_kernel(const phr_alignment* aln, uint64_t n_aln, uint64_t tlen, int depth,
+                                    uint32_t* track) {
+    const uint64_t a = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (a >= n_aln) return;
+    const uint32_t c = 1;
+    const uint32_t w = depth ? c : ((c + 2) / 5) * 5;
+    if (w == 0) return;
+    const uint64_t s0 = min(static_cast<uint64_t>(aln[a].target_start), tlen);
+    const uint64_t e0 = min(static_cast<uint64_t>(aln[a].target_end), tlen);
+    for (uint64_t p = s0 + lane; p < e0; p += 32) atomicAdd(track + p, w);
+}
+
 __global__ void offset_add_kernel(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t add) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i < n) out[i] = in[i] + add;
@@ -2102,6 +2119,78 @@ phr_status phr_align_reads_variants(phr_ctx* c, const phr_index* idx, const phr_
         return PHR_OK;
     }
     return phr::align_reads_host(ctx, idx, reads, *cfg, out, stats, vcfg, vout);
+}
+
+struct phr_coverage {
+    phr::Ctx* ctx = nullptr;
+    uint64_t tlen = 0;
+    int depth = 0;
+    uint32_t* d_track = nullptr;
+    phr_alignment* d_aln = nullptr;
+    uint64_t aln_cap = 0;
+};
+
+phr_status phr_coverage_create(phr_ctx* c, const phr_index* idx, phr_coverage_mode mode, phr_coverage** out) {
+    if (!c || !idx || !out || (mode != PHR_COVERAGE_QUANTIZED && mode != PHR_COVERAGE_DEPTH)) return PHR_ERR_ARG;
+    phr::Ctx* ctx = &c->impl;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    *out = nullptr;
+    phr_coverage* cv = new phr_coverage();
+    cv->ctx = ctx;
+    cv->tlen = idx->target_len;
+    cv->depth = mode == PHR_COVERAGE_DEPTH;
+    cudaError_t e = cudaMalloc(&cv->d_track, cv->tlen * 4 + 16);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cv->d_track, 0, cv->tlen * 4 + 16, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        if (cv->d_track) cudaFree(cv->d_track);
+        delete cv;
+        return phr::cuda_status(ctx, e, "coverage track");
+    }
+    *out = cv;
+    return PHR_OK;
+}
+
+phr_status phr_coverage_add(phr_coverage* cv, const phr_alignment* aln, uint64_t n_aln) {
+    if (!cv || (n_aln && !aln)) return PHR_ERR_ARG;
+    if (n_aln == 0) return PHR_OK;
+    phr::Ctx* ctx = cv->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    if (n_aln > cv->aln_cap) {
+        if (cv->d_aln) cudaFree(cv->d_aln);
+        cv->d_aln = nullptr;
+        cv->aln_cap = 0;
+        PHR_CUDA_TRY(ctx, cudaMalloc(&cv->d_aln, n_aln * sizeof(phr_alignment)));
+        cv->aln_cap = n_aln;
+    }
+    PHR_CUDA_TRY(ctx, cudaMemcpyAsync(cv->d_aln, aln, n_aln * sizeof(phr_alignment), cudaMemcpyHostToDevice, st));
+    {
+        phr::KernelScope ks(ctx, "coverage_add");
+        phr::coverage_add_kernel<<<phr::blocks_for(n_aln * 32, 256), 256, 0, st>>>(cv->d_aln, n_aln, cv->tlen,
+                                                                                  cv->depth, cv->d_track);
+    }
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return PHR_OK;
+}
+
+phr_status phr_coverage_read(phr_coverage* cv, uint32_t* track, uint64_t len) {
+    if (!cv || (len && !track) || len != cv->tlen) return PHR_ERR_ARG;
+    phr::Ctx* ctx = cv->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (len) PHR_CUDA_TRY(ctx, cudaMemcpy(track, cv->d_track, len * 4, cudaMemcpyDeviceToHost));
+    return PHR_OK;
+}
+
+void phr_coverage_destroy(phr_coverage* cv) {
+    if (!cv) return;
+    cudaSetDevice(cv->ctx->device);
+    if (cv->d_aln) cudaFree(cv->d_aln);
+    if (cv->d_track) cudaFree(cv->d_track);
+    delete cv;
 }
 
 phr_status phr_index_repeat_regions(const phr_index* idx, uint32_t* start, uint32_t* end, uint64_t cap, uint64_t* n) {

@@ -175,3 +175,21 @@ def test_variants_capacity_reports_needed_sizes(eng):
     assert st == A.PHR_ERR_CAPACITY
     _, _, _, _, off2, var2, cov2, al2 = eng.align_packed_variants(idx, packed, A.BALANCED, A.GAP_AFFINE)
     assert (va.variant_used, va.coverage_used, va.allele_used) == (len(var2), len(cov2), len(al2))
+
+
+@pytest.mark.parametrize("mode", [A.COVERAGE_QUANTIZED, A.COVERAGE_DEPTH], ids=["quantized", "depth"])
+def test_coverage_track_parity(eng, mode):
+    ref = str_target(100_000, 51)
+    target = ref + ref[2000:5000]
+    idx = eng.index(target)
+    track = eng.coverage_track(idx, mode)
+    exp = np.zeros(len(target), dtype=np.uint32)
+    for seed in (52, 53, 54):  # three batches merged into one resident track
+        packed = PackedReads(sim_reads(target, 400, 150, 0.02, seed) + sim_reads(target, 10, 2000, 0.03, seed))
+        rr, aln, cig, _ = eng.align_packed(idx, packed, A.SENSITIVE, A.GAP_AFFINE)
+        track.add(aln)
+        O.coverage_merge(aln, len(target), mode == A.COVERAGE_DEPTH, exp)
+    got = track.read()
+    assert np.array_equal(got, exp)
+    assert got.any() == (mode == A.COVERAGE_DEPTH)
+    track.close()

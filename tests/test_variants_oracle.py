@@ -202,3 +202,16 @@ def test_reference_local_coverage_windows():
     v = _local_coverage_case(b"ACGT" * 45, bytes(t))
     d = [x for x in v if x[0] == 75]
     assert d and len(d[0][8]) == 101 and all(c > 0 for c in d[0][8])
+
+
+def test_coverage_merge_quantized_track_is_zero_and_depth_counts():
+    # quantize_coverage(1) == ((1 + 2) / 5) * 5 == 0: per-read windows of count 1 merge to
+    # an all-zero track, as merge_result builds it; the depth mode counts the windows
+    aln = np.zeros(4, dtype=ALN_DTYPE)
+    aln["target_start"] = [0, 5, 90, 200]
+    aln["target_end"] = [10, 12, 120, 210]
+    assert not O.coverage_merge(aln, 100).any()
+    d = O.coverage_merge(aln, 100, depth=True)
+    assert d[:14].tolist() == [1] * 5 + [2] * 5 + [1, 1, 0, 0]
+    assert d[88:].tolist() == [0, 0] + [1] * 10
+    assert int(d.sum()) == 10 + 7 + 10
