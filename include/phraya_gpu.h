@@ -137,6 +137,8 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *   "wfa_big_smem"                       shared memory of that kernel, bytes (16 KiB..200 KiB)
  *   "max_blocks_per_sm"                  resident blocks per SM of the persistent extension
  *                                        kernels (1..4)
+ *   "host_chunks"                        chunks a host batch of more than 128 MiB of sequence
+ *                                        is copied and aligned in, overlapped (2..32, default 4)
  * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune
  * file (written by the autotuner); unknown keys and bad values there are ignored. */
 phr_status phr_ctx_set_tune(phr_ctx* ctx, const char* key, int64_t value);

@@ -290,10 +290,13 @@ phr_status extend_host(phr_ctx* c, phr_engine engine, const phr_pair_batch* batc
         const uint64_t bad = scan_host_batch(batch, &segs, 64);
         if (bad < n) return phr::set_error(ctx, PHR_ERR_ARG, "pair " + std::to_string(bad) + " reaches past seq_bytes");
     }
-    // batches of more than kChunkMin sequence bytes run in about four overlapped chunks
+    // batches of more than 2 kChunkMin sequence bytes run in about host_chunks overlapped
+    // chunks of at least 4 kChunkMin / host_chunks bytes
     constexpr uint64_t kChunkMin = 64ull << 20;
     if (batch->seq_bytes > 2 * kChunkMin) {
-        const std::vector<HostChunk> ch = plan_chunks(segs, std::max<uint64_t>(kChunkMin, batch->seq_bytes / 4));
+        const uint64_t nch = static_cast<uint64_t>(ctx->tune.host_chunks);
+        const std::vector<HostChunk> ch =
+            plan_chunks(segs, std::max<uint64_t>(4 * kChunkMin / nch, batch->seq_bytes / nch));
         uint64_t span = 0;
         for (const HostChunk& k : ch) span += k.hi - k.lo;
         // chunks whose pairs reference scattered bytes would copy more than the batch: one piece
@@ -379,6 +382,7 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "wfa_big_smem")) return &t.wfa_big_smem;
     if (!std::strcmp(key, "max_blocks_per_sm")) return &t.max_blocks_per_sm;
     if (!std::strcmp(key, "wfa_long_min")) return &t.wfa_long_min;
+    if (!std::strcmp(key, "host_chunks")) return &t.host_chunks;
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
@@ -391,6 +395,7 @@ bool tune_valid(const char* key, int64_t v) {
     if (!std::strcmp(key, "wfa_big_smem")) return v >= (16 << 10) && v <= (200 << 10) && v % 16 == 0;
     if (!std::strcmp(key, "max_blocks_per_sm")) return v >= 1 && v <= 4;
     if (!std::strcmp(key, "wfa_long_min")) return v >= 0 && v <= INT32_MAX;
+    if (!std::strcmp(key, "host_chunks")) return v >= 2 && v <= 32;
     return false;
 }
 }  // namespace

@@ -193,6 +193,19 @@ __device__ __forceinline__ uint32_t code2x4(uint32_t x, bool& pure) {
     return c & 0xFFu;
 }
 
+// code2x4 over the first `keep` (0..4) bytes of x only: the codes of the other bytes are
+// zero and they do not affect `pure`.
+__device__ __forceinline__ uint32_t code2x4m(uint32_t x, int keep, bool& pure) {
+    const uint32_t bytes = keep >= 4 ? 0xFFFFFFFFu : (1u << (8 * keep)) - 1u;
+    const uint32_t m = __vcmpeq4(x, 0x41414141u) | __vcmpeq4(x, 0x43434343u) | __vcmpeq4(x, 0x47474747u) |
+                       __vcmpeq4(x, 0x54545454u);
+    if ((m & bytes) != bytes) pure = false;
+    uint32_t c = ((x >> 1) ^ (x >> 2)) & 0x03030303u & bytes;
+    c |= c >> 6;
+    c |= c >> 12;
+    return c & 0xFFu;
+}
+
 // Writes "<n><op>" at p, returns its length.
 __device__ uint32_t write_count_op(char* p, uint32_t n, char op) {
     const uint32_t nd = ndigits(n);
@@ -296,15 +309,20 @@ __global__ void pack_kernel(PackParams P) {
         const int lim = min(16, len - p0);
         const uint8_t* cp = src + p0;
         const uintptr_t a0 = reinterpret_cast<uintptr_t>(cp) & ~static_cast<uintptr_t>(3);
-        if (wide && lim == 16 && a0 >= ok_lo && a0 + 20 <= ok_hi) {
-            // 16 bases from five aligned words, four bases per step
+        if (wide && a0 >= ok_lo && a0 + 20 <= ok_hi) {
+            // 16 bases from five aligned words, four bases per step; in the last word of a
+            // sequence the bytes past its end are read (inside the arena) but neither
+            // coded nor checked
             const uint32_t* wp = reinterpret_cast<const uint32_t*>(a0);
             const uint32_t sh = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(cp) & 3) * 8;
             uint32_t v[5];
 #pragma unroll
             for (int j = 0; j < 5; ++j) v[j] = __ldg(wp + j);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) word |= code2x4(__funnelshift_r(v[j], v[j + 1], sh), pure) << (8 * j);
+            for (int j = 0; j < 4; ++j) {
+                const int keep = min(max(lim - 4 * j, 0), 4);  // bytes of this group inside the sequence
+                word |= code2x4m(__funnelshift_r(v[j], v[j + 1], sh), keep, pure) << (8 * j);
+            }
         } else {
             for (int b = 0; b < lim; ++b) word |= code2(cp[b], pure) << (2 * b);
         }
@@ -411,42 +429,62 @@ __device__ __forceinline__ uint64_t myers_need_est(int m, int n, int G, int band
 
 __global__ void task_fill_kernel(TaskBuild T) {
     const uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
-    if (p >= T.n || !T.flag[p]) return;
-    const uint32_t k = T.keys[p];
-    const int G = key_group(k);
-    const uint32_t per = 32 / G;
-    uint32_t cnt = 0;
-    uint64_t need = 0, region = 0;
-    // lane-kernel tasks (global Myers, 2-bit, one lane per pair): window over the union band
-    const bool lane_task = T.engine == PHR_ENGINE_MYERS_GLOBAL && G == 1 && !((k >> 31) & 1);
-    int dmin = 0x7fffffff, dmax = static_cast<int>(0x80000000), n_max = 0, m_max = 0;
-    for (uint32_t c = 0; c < per && p + c < T.n; ++c) {
-        const uint32_t kc = T.keys[p + c];
-        if (kc == kInvalidKey || key_seg(kc) != key_seg(k)) break;
-        const PairDesc d = T.desc[T.order[p + c]];
-        if (lane_task) {
-            const LaneBand b = lane_band(d.qn, d.tn, T.band_base);
-            dmin = min(dmin, b.dmin);
-            dmax = max(dmax, b.dmax);
-            n_max = max(n_max, d.tn);
-            m_max = max(m_max, d.qn);
-        } else if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
-            need += myers_need_est(d.qn, d.tn, G, T.band_base);
-        else if (!big_pair(T.engine, T.big_min, T.big_smem, d.qn, d.tn, d.mode))
-            region = max(region, wfa_region_est(d.qn, d.tn, T.engine == PHR_ENGINE_WFA_AFFINE));
-        ++cnt;
+    // every lane stays to the warp-level reductions at the end; lanes without a task
+    // contribute nothing to them
+    const bool has_task = p < T.n && T.flag[p];
+    uint64_t need = 0;
+    uint32_t t_split = 0xFFFFFFFFu, t_g1 = 0xFFFFFFFFu;
+    if (has_task) {
+        const uint32_t k = T.keys[p];
+        const int G = key_group(k);
+        const uint32_t per = 32 / G;
+        uint32_t cnt = 0;
+        uint64_t region = 0;
+        // lane-kernel tasks (global Myers, 2-bit, one lane per pair): window over the union band
+        const bool lane_task = T.engine == PHR_ENGINE_MYERS_GLOBAL && G == 1 && !((k >> 31) & 1);
+        int dmin = 0x7fffffff, dmax = static_cast<int>(0x80000000), n_max = 0, m_max = 0;
+        for (uint32_t c = 0; c < per && p + c < T.n; ++c) {
+            const uint32_t kc = T.keys[p + c];
+            if (kc == kInvalidKey || key_seg(kc) != key_seg(k)) break;
+            const PairDesc d = T.desc[T.order[p + c]];
+            if (lane_task) {
+                const LaneBand b = lane_band(d.qn, d.tn, T.band_base);
+                dmin = min(dmin, b.dmin);
+                dmax = max(dmax, b.dmax);
+                n_max = max(n_max, d.tn);
+                m_max = max(m_max, d.qn);
+            } else if (T.engine == PHR_ENGINE_MYERS_FIT || T.engine == PHR_ENGINE_MYERS_GLOBAL)
+                need += myers_need_est(d.qn, d.tn, G, T.band_base);
+            else if (!big_pair(T.engine, T.big_min, T.big_smem, d.qn, d.tn, d.mode))
+                region = max(region, wfa_region_est(d.qn, d.tn, T.engine == PHR_ENGINE_WFA_AFFINE));
+            ++cnt;
+        }
+        if (T.engine != PHR_ENGINE_MYERS_FIT && T.engine != PHR_ENGINE_MYERS_GLOBAL) need = region * per;
+        if (lane_task && cnt) need = lane_task_need(n_max, m_max, lane_slots(dmin, dmax, (m_max + 63) >> 6));
+        const uint32_t t = T.tidx[p];
+        T.task_first[t] = static_cast<uint32_t>(p);
+        T.task_count[t] = static_cast<uint8_t>(cnt);
+        T.task_group[t] = static_cast<uint8_t>(G);
+        T.task_need[t] = need;
+        if ((k >> 31) & 1) t_split = t;
+        else if (G > 1) t_g1 = t;
     }
-    if (T.engine != PHR_ENGINE_MYERS_FIT && T.engine != PHR_ENGINE_MYERS_GLOBAL) need = region * per;
-    if (lane_task && cnt) need = lane_task_need(n_max, m_max, lane_slots(dmin, dmax, (m_max + 63) >> 6));
-    const uint32_t t = T.tidx[p];
-    T.task_first[t] = static_cast<uint32_t>(p);
-    T.task_count[t] = static_cast<uint8_t>(cnt);
-    T.task_group[t] = static_cast<uint8_t>(G);
-    T.task_need[t] = need;
-    if (need) atomicAdd(&T.need_hist[64 - __clzll(need)], 1u);
-    atomicMax(T.need_max, static_cast<unsigned long long>(need));
-    if ((k >> 31) & 1) atomicMin(T.split_min, t);
-    else if (G > 1) atomicMin(T.g1_min, t);
+    // one atomic per warp and value instead of one per task (a million tasks would
+    // otherwise queue on the same three addresses)
+    uint64_t nmax = need;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nmax = max(nmax, __shfl_xor_sync(PHR_FULL_MASK, nmax, o));
+    t_split = __reduce_min_sync(PHR_FULL_MASK, t_split);
+    t_g1 = __reduce_min_sync(PHR_FULL_MASK, t_g1);
+    const int bucket = need ? 64 - __clzll(need) : 64;   // 64: no histogram entry
+    const uint32_t same = __match_any_sync(PHR_FULL_MASK, bucket);
+    const int lane = threadIdx.x & 31;
+    if (bucket < 64 && lane == __ffs(same) - 1) atomicAdd(&T.need_hist[bucket], static_cast<unsigned>(__popc(same)));
+    if (lane == 0) {
+        if (nmax) atomicMax(T.need_max, static_cast<unsigned long long>(nmax));
+        if (t_split != 0xFFFFFFFFu) atomicMin(T.split_min, t_split);
+        if (t_g1 != 0xFFFFFFFFu) atomicMin(T.g1_min, t_g1);
+    }
 }
 
 __global__ void task_finalize_kernel(TaskBuild T) {

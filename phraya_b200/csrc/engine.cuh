@@ -42,6 +42,7 @@ struct EngineTune {
     int wfa_big_min = 4096;          // linear WFA pairs with qn+tn >= this run one per CTA (0: off)
     int wfa_big_smem = 100 << 10;    // shared memory of that kernel, bytes (two CTAs per SM)
     int max_blocks_per_sm = 4;       // resident blocks per SM of the persistent extension kernels
+    int host_chunks = 4;             // chunks a large host batch is copied and aligned in (overlapped)
 };
 
 struct Ctx {

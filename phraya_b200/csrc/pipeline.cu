@@ -15,6 +15,8 @@
 // duplicates emitted once; pairs are (key, k-mer start).
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
+#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/iterator/counting_input_iterator.cuh>
 #include <cub/device/device_segmented_sort.cuh>
 
@@ -1000,6 +1002,40 @@ __global__ void coverage_add_kernel(const phr_alignment* aln, uint64_t n_aln, ui
     for (uint64_t p = s0 + lane; p < e0; p += 32) atomicAdd(track + p, w);
 }
 
+// ---------------------------------------------------------------------------
+// Minimizer index build (build_minimizer_index, seeding.rs:31-37)
+// ---------------------------------------------------------------------------
+__global__ void iota_u32_kernel(uint32_t* out, uint64_t n) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i < n) out[i] = static_cast<uint32_t>(i);
+}
+
+// Positions grouped by value: the stable sort by value kept each value's entries in
+// sketch order, which is the order of its position list.
+__global__ void gather_pos_kernel(const uint32_t* pos, const uint32_t* order, uint64_t n, uint32_t* out) {
+    const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (i < n) out[i] = pos[order[i]];
+}
+
+// Open addressing, linear probing from value & mask (the lookup's probe sequence). A slot
+// is claimed by swapping its count from 0 (counts are at least 1); the table has at least
+// twice as many slots as values, so the probe ends; it is bounded by the table size.
+__global__ void index_insert_kernel(const uint64_t* uniq, const uint32_t* run_cnt, const uint32_t* run_off,
+                                    const int* n_runs, uint64_t mask, uint64_t* keys, uint32_t* off, uint32_t* cnt) {
+    const uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
+    if (r >= static_cast<uint64_t>(*n_runs)) return;
+    const uint64_t v = uniq[r];
+    uint64_t s = v & mask;
+    for (uint64_t probe = 0; probe <= mask; ++probe) {
+        if (atomicCAS(cnt + s, 0u, run_cnt[r]) == 0u) {
+            keys[s] = v;
+            off[s] = run_off[r];
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+}
+
 __global__ void offset_add_kernel(const uint64_t* in, uint64_t* out, uint64_t n, uint64_t add) {
     const uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x;
     if (i < n) out[i] = in[i] + add;
@@ -1123,56 +1159,89 @@ phr_status sketch_device(Ctx* ctx, DeviceArena& A, const uint8_t* seq, const uin
 }
 
 // Builds the device index from a host sketch (build_minimizer_index + occurrence cap).
-static phr_status build_index_from_sketch(Ctx* ctx, phr_index* idx, const uint64_t* vals, const uint32_t* pos,
-                                          uint64_t n) {
-    std::unordered_map<uint64_t, std::vector<uint32_t>> map;
-    map.reserve(n * 2 + 16);
-    std::vector<uint64_t> order;  // first-appearance order of values (deterministic layout)
-    for (uint64_t i = 0; i < n; ++i) {
-        auto it = map.find(vals[i]);
-        if (it == map.end()) {
-            order.push_back(vals[i]);
-            map[vals[i]].push_back(pos[i]);
-        } else {
-            it->second.push_back(pos[i]);
+// build_minimizer_index (seeding.rs:31-37) and seed_occurrence_cap (seeding.rs:94-102,
+// floor 256, executor.rs:258) on the device from a sketch already on the device: a stable
+// radix sort of (value, entry) pairs groups each value's positions in sketch order, a
+// run-length encoding gives the distinct values and their counts, the median count sets
+// the cap, and the values go into an open-addressing table. Temporaries live in the
+// context's extension arena; the index itself is one allocation kept by `idx`.
+static phr_status build_index_device(Ctx* ctx, phr_index* idx, const uint64_t* vals, const uint32_t* pos, uint64_t n) {
+    cudaStream_t st = ctx->stream;
+    const unsigned T = 256;
+    if (n > 0x7FFFFFF0ull) return set_error(ctx, PHR_ERR_ARG, "sketch of more than 2^31 - 16 minimizers");
+    const int ni = static_cast<int>(n);
+    DeviceArena& A = ctx->arena;
+    A.reset();
+    size_t t_sort = 0, t_rle = 0, t_scan = 0, t_csort = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t_sort, static_cast<const uint64_t*>(nullptr),
+                                    static_cast<uint64_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                    static_cast<uint32_t*>(nullptr), ni, 0, 64, st);
+    cub::DeviceRunLengthEncode::Encode(nullptr, t_rle, static_cast<const uint64_t*>(nullptr),
+                                       static_cast<uint64_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                       static_cast<int*>(nullptr), ni, st);
+    cub::DeviceScan::ExclusiveSum(nullptr, t_scan, static_cast<const uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), ni, st);
+    cub::DeviceRadixSort::SortKeys(nullptr, t_csort, static_cast<const uint32_t*>(nullptr),
+                                   static_cast<uint32_t*>(nullptr), ni, 0, 32, st);
+    const size_t t_need = std::max({t_sort, t_rle, t_scan, t_csort}) + 256;
+    auto al = [](size_t b) { return (b + 511) / 256 * 256; };
+    PHR_CUDA_TRY(ctx, A.reserve(al(n * 8) * 2 + al(n * 4) * 6 + al(64) + al(t_need) + 4096));
+    uint64_t* skeys = static_cast<uint64_t*>(A.take(n * 8 + 8));
+    uint64_t* uniq = static_cast<uint64_t*>(A.take(n * 8 + 8));
+    uint32_t* ent = static_cast<uint32_t*>(A.take(n * 4 + 8));
+    uint32_t* order = static_cast<uint32_t*>(A.take(n * 4 + 8));
+    uint32_t* run_cnt = static_cast<uint32_t*>(A.take(n * 4 + 8));
+    uint32_t* run_off = static_cast<uint32_t*>(A.take(n * 4 + 8));
+    uint32_t* cnt_sorted = static_cast<uint32_t*>(A.take(n * 4 + 8));
+    int* d_runs = static_cast<int*>(A.take(64));
+    void* tmp = A.take(t_need);
+    if (!tmp) return set_error(ctx, PHR_ERR_OOM, "arena exhausted (index build)");
+    int h_runs = 0;
+    uint32_t h_median = 0;
+    if (n) {
+        {
+            KernelScope ks(ctx, "index_iota");
+            iota_u32_kernel<<<blocks_for(n, T), T, 0, st>>>(ent, n);
         }
+        size_t t = t_need;
+        cub::DeviceRadixSort::SortPairs(tmp, t, vals, skeys, ent, order, ni, 0, 64, st);
+        t = t_need;
+        cub::DeviceRunLengthEncode::Encode(tmp, t, skeys, uniq, run_cnt, d_runs, ni, st);
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_runs, d_runs, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        t = t_need;
+        cub::DeviceScan::ExclusiveSum(tmp, t, run_cnt, run_off, h_runs, st);
+        t = t_need;
+        cub::DeviceRadixSort::SortKeys(tmp, t, run_cnt, cnt_sorted, h_runs, 0, 32, st);
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&h_median, cnt_sorted + h_runs / 2, 4, cudaMemcpyDeviceToHost, st));
     }
-    // seed_occurrence_cap (seeding.rs:94-102), floor 256 (executor.rs:258)
-    uint64_t cap = 256;
-    if (!map.empty()) {
-        std::vector<uint64_t> counts;
-        counts.reserve(map.size());
-        for (auto& kv : map) counts.push_back(kv.second.size());
-        std::sort(counts.begin(), counts.end());
-        cap = std::max<uint64_t>(256, counts[counts.size() / 2] * 8);
-    }
+    const uint64_t distinct = static_cast<uint64_t>(h_runs);
     uint64_t slots = 16;
-    while (slots < 2 * map.size() + 16) slots <<= 1;
-    std::vector<uint64_t> hkeys(slots, 0);
-    std::vector<uint32_t> hoff(slots, 0), hcnt(slots, 0), hpos;
-    hpos.reserve(n);
-    for (uint64_t v : order) {
-        const auto& ps = map[v];
-        uint64_t s = v & (slots - 1);
-        while (hcnt[s] != 0) s = (s + 1) & (slots - 1);
-        hkeys[s] = v;
-        hoff[s] = static_cast<uint32_t>(hpos.size());
-        hcnt[s] = static_cast<uint32_t>(ps.size());
-        hpos.insert(hpos.end(), ps.begin(), ps.end());
-    }
-    const size_t bytes = slots * (8 + 4 + 4) + hpos.size() * 4 + 256;
+    while (slots < 2 * distinct + 16) slots <<= 1;
+    const size_t bytes = slots * (8 + 4 + 4) + n * 4 + 256;
     void* blk = nullptr;
     PHR_CUDA_TRY(ctx, cudaMalloc(&blk, bytes));
+    idx->d_block = blk;
     char* p = static_cast<char*>(blk);
     uint64_t* keys = reinterpret_cast<uint64_t*>(p);
     uint32_t* off = reinterpret_cast<uint32_t*>(p + slots * 8);
     uint32_t* cnt = reinterpret_cast<uint32_t*>(p + slots * 12);
     uint32_t* dpos = reinterpret_cast<uint32_t*>(p + slots * 16);
-    idx->d_block = blk;
-    PHR_CUDA_TRY(ctx, cudaMemcpy(keys, hkeys.data(), slots * 8, cudaMemcpyHostToDevice));
-    PHR_CUDA_TRY(ctx, cudaMemcpy(off, hoff.data(), slots * 4, cudaMemcpyHostToDevice));
-    PHR_CUDA_TRY(ctx, cudaMemcpy(cnt, hcnt.data(), slots * 4, cudaMemcpyHostToDevice));
-    if (!hpos.empty()) PHR_CUDA_TRY(ctx, cudaMemcpy(dpos, hpos.data(), hpos.size() * 4, cudaMemcpyHostToDevice));
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(keys, 0, slots * 8, st));
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(off, 0, slots * 4, st));
+    PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, slots * 4, st));
+    if (n) {
+        {
+            KernelScope ks(ctx, "index_gather");
+            gather_pos_kernel<<<blocks_for(n, T), T, 0, st>>>(pos, order, n, dpos);
+        }
+        KernelScope ks(ctx, "index_insert");
+        index_insert_kernel<<<blocks_for(distinct, T), T, 0, st>>>(uniq, run_cnt, run_off, d_runs, slots - 1, keys, off,
+                                                                  cnt);
+    }
+    PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    PHR_CUDA_TRY(ctx, cudaGetLastError());
+    const uint64_t cap = distinct ? std::max<uint64_t>(256, static_cast<uint64_t>(h_median) * 8) : 256;
     idx->view.keys = keys;
     idx->view.off = off;
     idx->view.cnt = cnt;
@@ -1180,7 +1249,7 @@ static phr_status build_index_from_sketch(Ctx* ctx, phr_index* idx, const uint64
     idx->view.mask = slots - 1;
     idx->view.occ_cap = static_cast<uint32_t>(std::min<uint64_t>(cap, 0xFFFFFFFFu));
     idx->n_min = n;
-    idx->n_distinct = map.size();
+    idx->n_distinct = distinct;
     idx->device_bytes = bytes + idx->target_len + 64;
     return PHR_OK;
 }
@@ -1280,20 +1349,38 @@ phr_status index_create(Ctx* ctx, const uint8_t* target, uint64_t tlen, const ph
             return cuda_status(ctx, e, "cudaMemcpy(target)");
         }
     }
-    std::vector<uint64_t> hv;
-    std::vector<uint32_t> hp;
+    DeviceArena& A = ctx->pipe;
+    A.reset();
+    const uint64_t* d_vals = nullptr;
+    const uint32_t* d_pos = nullptr;
+    uint64_t total = 0;
     if (sketch) {
         if (sketch->n && (!sketch->values || !sketch->positions)) {
             delete idx;
             return set_error(ctx, PHR_ERR_ARG, "sketch arrays are NULL");
         }
-        hv.assign(sketch->values, sketch->values + sketch->n);
-        hp.assign(sketch->positions, sketch->positions + sketch->n);
         if (sketch->k > 0) idx->k = sketch->k;
         if (sketch->w > 0) idx->w = sketch->w;
+        total = sketch->n;
+        e = A.reserve(total * 12 + 4096);
+        uint64_t* v = static_cast<uint64_t*>(A.take(total * 8 + 8));
+        uint32_t* q = static_cast<uint32_t*>(A.take(total * 4 + 8));
+        if (e != cudaSuccess || !q) {
+            delete idx;
+            return e != cudaSuccess ? cuda_status(ctx, e, "arena reserve (sketch upload)")
+                                    : set_error(ctx, PHR_ERR_OOM, "arena exhausted (sketch upload)");
+        }
+        if (total) {
+            e = cudaMemcpyAsync(v, sketch->values, total * 8, cudaMemcpyHostToDevice, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(q, sketch->positions, total * 4, cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) {
+                delete idx;
+                return cuda_status(ctx, e, "sketch upload");
+            }
+        }
+        d_vals = v;
+        d_pos = q;
     } else {
-        DeviceArena& A = ctx->pipe;
-        A.reset();
         e = A.reserve(tlen * 40 + (64 << 20));
         if (e != cudaSuccess) {
             delete idx;
@@ -1307,26 +1394,16 @@ phr_status index_create(Ctx* ctx, const uint8_t* target, uint64_t tlen, const ph
         cudaMemcpy(len, &l32, 4, cudaMemcpyHostToDevice);
         uint64_t *vals = nullptr, *sk_off = nullptr;
         uint32_t *poss = nullptr, *sk_n = nullptr;
-        uint64_t total = 0;
         phr_status s = sketch_device(ctx, A, idx->d_target, off, len, 1, idx->k, idx->w, alphabet, &vals, &poss,
                                      &sk_off, &sk_n, &total, nullptr);
         if (s != PHR_OK) {
             delete idx;
             return s;
         }
-        hv.resize(total);
-        hp.resize(total);
-        if (total) {
-            cudaMemcpyAsync(hv.data(), vals, total * 8, cudaMemcpyDeviceToHost, ctx->stream);
-            cudaMemcpyAsync(hp.data(), poss, total * 4, cudaMemcpyDeviceToHost, ctx->stream);
-        }
-        e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) {
-            delete idx;
-            return cuda_status(ctx, e, "target sketch");
-        }
+        d_vals = vals;
+        d_pos = poss;
     }
-    phr_status s = build_index_from_sketch(ctx, idx, hv.data(), hp.data(), hv.size());
+    phr_status s = build_index_device(ctx, idx, d_vals, d_pos, total);
     if (s == PHR_OK) s = detect_repeats(ctx, idx, target);
     if (s != PHR_OK) {
         delete idx;

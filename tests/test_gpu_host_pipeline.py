@@ -47,3 +47,15 @@ def test_chunked_host_batch_equals_device_call(engine, costs):
         da, dc = _device_call(eng, engine, packed, costs)
     assert np.array_equal(ha, da)
     assert bytes(hc) == dc
+
+
+@pytest.mark.parametrize("chunks", [2, 16])
+def test_chunk_count_does_not_change_results(chunks):
+    """host_chunks only changes how a host batch is split and overlapped."""
+    packed = D.to_packed(D.extension_pairs_device(450_000, 100, 300, 0.05, seed=43))
+    with P.Engine(0) as eng:
+        eng.set_tune("host_chunks", chunks)
+        ha, hc = eng.extend_packed(A.ENGINE_WFA_LINEAR, packed, P.AffineCosts(2, 4, 1))
+        da, dc = _device_call(eng, A.ENGINE_WFA_LINEAR, packed, (2, 4, 1))
+    assert np.array_equal(ha, da)
+    assert bytes(hc) == dc

@@ -58,6 +58,47 @@ def test_seed_chain_parity(eng):
         assert chains == exp
 
 
+def _seed_parity(eng, idx, tv, tp, reads):
+    cap = O.occurrence_cap(tv, tp)
+    assert idx.info()["occurrence_cap"] == cap
+    sks = [O.sketch(r) for r in reads]
+    for (v, p), (nseed, chains) in zip(sks, eng.seed_chain(idx, sks)):
+        seeds = O.find_seeds(tv, tp, v, p, cap)
+        assert nseed == len(seeds)
+        assert chains == O.chain_seeds(seeds)
+
+
+def test_index_build_on_device(eng):
+    # build_minimizer_index + seed_occurrence_cap from the device's own sketch and from a
+    # caller sketch; a repeated unit makes the median occurrence count (and so the cap)
+    # exceed the floor of 256
+    unit = D.random_reference(3000, seed=61)
+    target = D.random_reference(500, seed=62) + unit * 120 + D.random_reference(300, seed=63)
+    tv, tp = O.sketch(target)
+    reads = [target[s:s + 150] for s in range(0, len(target) - 150, 9973)] + [unit[100:400], target[:400]]
+    idx = eng.index(target)
+    inf = idx.info()
+    assert inf["n_minimizers"] == len(tv) and inf["n_distinct"] == len(np.unique(tv))
+    assert inf["occurrence_cap"] > 256
+    _seed_parity(eng, idx, tv, tp, reads)
+    idx.close()
+    # caller sketch: the device sketch's entries with a few positions moved, so the
+    # position lists come from the caller's arrays, in the caller's order
+    cv, cp = tv.copy(), tp.copy()
+    cp[::7] = (cp[::7] + 3) % len(target)
+    idx = eng.index(target, sketch=(cv, cp))
+    assert idx.info()["n_distinct"] == len(np.unique(cv))
+    _seed_parity(eng, idx, cv, cp, reads)
+    idx.close()
+    # empty sketch and a target shorter than k
+    for t, sk in ((target[:5000], (np.zeros(0, np.uint64), np.zeros(0, np.uint32))), (b"ACGTACGT", None)):
+        idx = eng.index(t, sketch=sk)
+        inf = idx.info()
+        assert inf["n_minimizers"] == 0 and inf["n_distinct"] == 0 and inf["occurrence_cap"] == 256
+        assert eng.seed_chain(idx, [O.sketch(target[:150])])[0][0] == 0
+        idx.close()
+
+
 def compare_reads(eng, target, reads, strat, gap, stored=None, alphabet=A.ALPHABET_DNA):
     idx = eng.index(target, alphabet)
     otg = O.Target(target, alphabet)

@@ -47,3 +47,12 @@ def test_tune_and_tune_file(tmp_path):
     with P.Engine(0, tune_file=str(path)) as e2:
         for k, v in values.items():
             assert e2.get_tune(k) == v
+
+
+def test_host_chunks_refuses_out_of_range_values():
+    with P.Engine(0) as eng:
+        for key, bad in (("host_chunks", 1), ("host_chunks", 33)):
+            with pytest.raises(P.EngineError):
+                eng.set_tune(key, bad)
+        eng.set_tune("host_chunks", 8)
+        assert eng.get_tune("host_chunks") == 8
