@@ -372,6 +372,13 @@ def run_engine(args, rank, world):
              for k in ("myers_lane", "wfa_affine", "wfa_linear") if k in kms}
     pipe = None
     if not args.no_pipeline:
+        # the read pipeline and the server start from a fresh context and an empty torch
+        # cache: the extension bench's arenas and buffers would otherwise hold device
+        # memory that the server's admission control waits for
+        del jobs
+        eng.close()
+        torch.cuda.empty_cache()
+        eng = P.Engine(dev)
         pipe = run_pipeline(eng, dev, args)
     cpu = cpu_baseline(set_a, set_b, n_a, n_b, os.cpu_count() or 1) if not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
@@ -470,9 +477,12 @@ def run_pipeline(eng, dev, args):
         gaps = np.random.default_rng(104).exponential(1.0 / rate, len(stream))
         arrive = np.cumsum(gaps)
         srv = eng.server(idx, strategy=A.BALANCED, max_batch_reads=2048, max_wait_us=1000, n_streams=3)
-        srv.submit_many(stream[:64])  # warm the workers
+        # warm the workers with a slice of the same mix (long reads included), so every
+        # worker's first long batch is behind it
+        warm = stream[:512]
+        srv.submit_many(warm)
         got = 0
-        while got < 64:
+        while got < len(warm):
             got += len(srv.poll(4096, wait_us=20000))
         lat = {}
         ids = {}

@@ -556,6 +556,10 @@ typedef struct {
     double latency_us;             /* submit -> result ready */
 } phr_server_result;
 
+/* While a server exists, the device's default CUDA memory pool keeps memory freed to it
+ * (release threshold raised to the maximum; the previous value is restored by
+ * phr_server_destroy), so the workers' arenas can grow again without the driver mapping
+ * memory while other workers' kernels run. */
 phr_status phr_server_create(phr_ctx* ctx, const phr_index* idx, const phr_server_config* cfg,
                              phr_server** out);
 /* Enqueues one read (bytes copied); returns its request id in *request_id. */

@@ -85,6 +85,10 @@ struct phr_server {
     uint64_t in_flight = 0;            // submitted, not yet completed
     uint64_t completions = 0;          // batches finished (admission waits on it)
     bool stopping = false;
+    // the device's default memory pool and its release threshold before this server
+    // raised it (restored at destroy)
+    cudaMemPool_t pool = nullptr;
+    uint64_t pool_threshold = 0;
     bool short_lane = false;
     phr_status fatal = PHR_OK;
     std::string fatal_msg;
@@ -275,15 +279,19 @@ void run_scheduler(phr_server* S) {
             batch.push_back(std::move(S->pending[b].front()));
             S->pending[b].pop_front();
         }
-        // admission by free HBM: wait while a batch this size does not fit
-        size_t free_b = 0, total_b = 0;
-        lk.unlock();
-        cudaMemGetInfo(&free_b, &total_b);
-        lk.lock();
+        // admission by free HBM: wait while a batch this size does not fit. The short lane
+        // skips it: its arenas were sized for a full short batch at creation, and a query
+        // of free memory can wait on another worker's allocator work.
+        size_t free_b = SIZE_MAX, total_b = 0;
+        if (!W->short_only) {
+            lk.unlock();
+            cudaMemGetInfo(&free_b, &total_b);
+            lk.lock();
+        }
         const uint64_t need = batch_need(batch.size(), bases);
         const bool others_busy =
             std::any_of(S->workers.begin(), S->workers.end(), [](auto* w) { return w->busy; });
-        if (free_b < need + S->cfg.hbm_reserve_bytes && others_busy) {
+        if (!W->short_only && free_b < need + S->cfg.hbm_reserve_bytes && others_busy) {
             // put the batch back (front, same order) and wait for a worker to finish
             for (auto it = batch.rbegin(); it != batch.rend(); ++it) S->pending[b].push_front(std::move(*it));
             const uint64_t seen = S->completions;
@@ -335,6 +343,17 @@ phr_status phr_server_create(phr_ctx* c, const phr_index* idx, const phr_server_
     int prio_low = 0, prio_high = 0;
     cudaSetDevice(c->impl.device);
     cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+    // workers' arenas grow and shrink through the device's default memory pool; keeping
+    // freed memory in the pool (no release threshold) spares them unmapping and mapping it
+    // again while other workers run
+    if (cudaDeviceGetDefaultMemPool(&S->pool, c->impl.device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        S->pool = nullptr;
+    }
+    cudaGetLastError();
     for (uint32_t w = 0; w < S->cfg.n_streams; ++w) {
         auto* W = new phr_server::Worker();
         W->ctx.device = c->impl.device;
@@ -464,6 +483,7 @@ phr_status phr_server_destroy(phr_server* S) {
         cudaStreamSynchronize(W->ctx.stream);
         delete W;
     }
+    if (S->pool) cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold);
     delete S;
     return st;
 }
