@@ -549,47 +549,57 @@ __global__ void text_len_kernel(const PairOut* out, uint64_t n, uint64_t* len) {
     len[i] = (o.status == PHR_OK) ? o.text_len : 0;
 }
 
-// Packs CIGAR text and writes the phr_alignment records. One warp per pair.
+// Packs CIGAR text and writes the phr_alignment records. One warp per 32 consecutive
+// pairs: lane l writes pair first + l's record (the warp's records are contiguous), then
+// the lanes copy the pairs' texts one pair after the other.
 __global__ void finish_kernel(FinishParams F) {
-    const uint64_t warp = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5;
+    const uint64_t first = ((blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) >> 5) * 32;
     const int lane = threadIdx.x & 31;
-    if (warp >= F.n) return;
-    const uint64_t i = warp;
-    const PairOut o = F.out[i];
-    const PairDesc d = F.desc[i];
-    const uint64_t off = F.cig_off[i];
-    const uint32_t len = (o.status == PHR_OK) ? o.text_len : 0;
-    if (o.status == -1) {
-        if (lane == 0) atomicOr(F.error_flag, 8u);
-        return;
-    }
-    if (off + len <= F.cigar_capacity) {
-        const char* src = F.text + F.text_off[i];
-        for (uint32_t c = lane; c < len; c += 32) F.cigar[off + c] = src[c];
-    } else if (lane == 0) {
-        atomicOr(F.error_flag, 16u);
-    }
-    if (lane == 0) {
-        phr_alignment a;
-        a.status = o.status;
-        a.edit_distance = o.status == PHR_OK ? static_cast<uint32_t>(o.ed) : 0;
-        a.cigar_off = F.cigar_base + off;
-        a.cigar_len = len;
-        a.affine_score = o.status == PHR_OK ? static_cast<uint32_t>(o.affine_score) : 0;
-        if (F.engine == PHR_ENGINE_MYERS_GLOBAL) {
-            a.query_start = 0;
-            a.query_end = static_cast<uint32_t>(d.qn);
-            a.target_start = 0;
-            a.target_end = static_cast<uint32_t>(d.tn);
-        } else if (o.status == PHR_INVALID_INPUT || o.status == PHR_ALIGNMENT_FAILED) {
-            a.query_start = a.query_end = a.target_start = a.target_end = 0;
+    if (first >= F.n) return;
+    const uint64_t i = first + lane;
+    uint64_t off = 0, toff = 0;
+    uint32_t len = 0;
+    bool copy = false;
+    if (i < F.n) {
+        const PairOut o = F.out[i];
+        if (o.status == -1) {
+            atomicOr(F.error_flag, 8u);
         } else {
-            a.query_start = static_cast<uint32_t>(d.qs);
-            a.query_end = static_cast<uint32_t>(d.qs + d.qn);
-            a.target_start = static_cast<uint32_t>(d.ts);
-            a.target_end = static_cast<uint32_t>(d.ts + o.t_consumed);
+            const PairDesc d = F.desc[i];
+            off = F.cig_off[i];
+            toff = F.text_off[i];
+            len = (o.status == PHR_OK) ? o.text_len : 0;
+            copy = off + len <= F.cigar_capacity;
+            if (!copy) atomicOr(F.error_flag, 16u);
+            phr_alignment a;
+            a.status = o.status;
+            a.edit_distance = o.status == PHR_OK ? static_cast<uint32_t>(o.ed) : 0;
+            a.cigar_off = F.cigar_base + off;
+            a.cigar_len = len;
+            a.affine_score = o.status == PHR_OK ? static_cast<uint32_t>(o.affine_score) : 0;
+            if (F.engine == PHR_ENGINE_MYERS_GLOBAL) {
+                a.query_start = 0;
+                a.query_end = static_cast<uint32_t>(d.qn);
+                a.target_start = 0;
+                a.target_end = static_cast<uint32_t>(d.tn);
+            } else if (o.status == PHR_INVALID_INPUT || o.status == PHR_ALIGNMENT_FAILED) {
+                a.query_start = a.query_end = a.target_start = a.target_end = 0;
+            } else {
+                a.query_start = static_cast<uint32_t>(d.qs);
+                a.query_end = static_cast<uint32_t>(d.qs + d.qn);
+                a.target_start = static_cast<uint32_t>(d.ts);
+                a.target_end = static_cast<uint32_t>(d.ts + o.t_consumed);
+            }
+            F.aln[i] = a;
         }
-        F.aln[i] = a;
+    }
+    const unsigned todo = __ballot_sync(PHR_FULL_MASK, copy && len > 0);
+    for (unsigned m = todo; m; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        const uint32_t lj = __shfl_sync(PHR_FULL_MASK, len, j);
+        const uint64_t oj = __shfl_sync(PHR_FULL_MASK, off, j);
+        const uint64_t tj = __shfl_sync(PHR_FULL_MASK, toff, j);
+        for (uint32_t c = lane; c < lj; c += 32) F.cigar[oj + c] = F.text[tj + c];
     }
 }
 
@@ -1012,7 +1022,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                    res->cigar_capacity, cnt + 10, res->cigar_base};
     {
         KernelScope ks(ctx, "finish");
-        finish_kernel<<<blocks_for(n * 32, T), T, 0, st>>>(F);
+        finish_kernel<<<blocks_for((n + 31) / 32 * 32, T), T, 0, st>>>(F);
     }
     uint32_t h_err = 0;
     unsigned long long h_work[4] = {0, 0, 0, 0};

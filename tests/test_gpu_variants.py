@@ -96,9 +96,9 @@ def test_repeat_regions_protein_index(eng):
     assert idx.repeat_regions() == O.tandem_repeats(bytes(t))
 
 
-def compare_variants(eng, target, reads, strat, gap, radius=0, hotspots=(), stored=None):
-    idx = eng.index(target)
-    otg = O.Target(target)
+def compare_variants(eng, target, reads, strat, gap, radius=0, hotspots=(), stored=None, alphabet=A.ALPHABET_DNA):
+    idx = eng.index(target, alphabet)
+    otg = O.Target(target, alphabet)
     packed = PackedReads(reads, stored)
     rr, aln, cig, st, off, var, cov, al = eng.align_packed_variants(idx, packed, strat, gap, radius, hotspots)
     # the alignments are phr_align_reads' own
@@ -152,6 +152,32 @@ def test_variants_parity_radius_and_scenarios(eng):
     t = bytearray(b"A" * 150)
     t[149] = ord("T")
     compare_variants(eng, bytes(t), [b"A" * 150], A.BALANCED, A.GAP_AFFINE)
+
+
+def test_variants_parity_protein(eng):
+    rng = np.random.default_rng(71)
+    alph = list(b"ACDEFGHIKLMNPQRSTVWY")
+    target = bytearray(rng.choice(alph, 30000).tolist())
+    target[5000:5024] = b"QQQQ" * 6  # a tandem repeat on the protein index too
+    target = bytes(target)
+    reads = []
+    for _ in range(150):
+        p = int(rng.integers(0, len(target) - 400))
+        r = bytearray(target[p:p + int(rng.integers(150, 400))])
+        for _ in range(int(rng.integers(0, 12))):
+            j = int(rng.integers(0, len(r)))
+            u = rng.random()
+            if u < 0.6:
+                r[j] = int(rng.choice(alph))
+            elif u < 0.8:
+                r[j:j] = bytes(rng.choice(alph, int(rng.integers(1, 4))).tolist())
+            else:
+                del r[j:j + int(rng.integers(1, 4))]
+        reads.append(bytes(r))
+    for strat, gap in ((A.BALANCED, A.GAP_AFFINE), (A.SENSITIVE, A.GAP_AFFINE)):
+        off, var, cov, al = compare_variants(eng, target, reads, strat, gap, hotspots=[(4000, 6000)],
+                                             alphabet=A.ALPHABET_PROTEIN)
+        assert len(var) > 100 and set(var["strand"].tolist()) == {0}
 
 
 def test_variants_capacity_reports_needed_sizes(eng):
