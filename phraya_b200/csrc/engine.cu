@@ -180,30 +180,20 @@ __device__ __forceinline__ uint32_t code2(uint8_t b, bool& pure) {
     }
 }
 
-// Four ASCII bytes -> their 2-bit codes (A, C, G, T = 0..3) in the low 8 bits; `pure`
-// turns false unless all four bytes are A, C, G or T. The code of A/C/G/T is bits 1-2
-// of the byte XOR bits 2-3 (0x41, 0x43, 0x47, 0x54 -> 0, 1, 2, 3).
-__device__ __forceinline__ uint32_t code2x4(uint32_t x, bool& pure) {
-    const uint32_t m = __vcmpeq4(x, 0x41414141u) | __vcmpeq4(x, 0x43434343u) | __vcmpeq4(x, 0x47474747u) |
-                       __vcmpeq4(x, 0x54545454u);
-    if (m != 0xFFFFFFFFu) pure = false;
-    uint32_t c = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
-    c |= c >> 6;
-    c |= c >> 12;
-    return c & 0xFFu;
-}
-
-// code2x4 over the first `keep` (0..4) bytes of x only: the codes of the other bytes are
-// zero and they do not affect `pure`.
+// The first `keep` (0..4) of four ASCII bytes -> their 2-bit codes (A, C, G, T = 0..3) in
+// the low 8 bits (the other bytes' codes are zero); `pure` turns false unless those bytes
+// are all A, C, G or T. The code of A/C/G/T is bits 1-2 of the byte XOR bits 2-3 (0x41,
+// 0x43, 0x47, 0x54 -> 0, 1, 2, 3); a byte is one of them exactly when the letter of its
+// code ('A', 'C', 'G', 'T' picked by one byte permute) is the byte itself.
 __device__ __forceinline__ uint32_t code2x4m(uint32_t x, int keep, bool& pure) {
     const uint32_t bytes = keep >= 4 ? 0xFFFFFFFFu : (1u << (8 * keep)) - 1u;
-    const uint32_t m = __vcmpeq4(x, 0x41414141u) | __vcmpeq4(x, 0x43434343u) | __vcmpeq4(x, 0x47474747u) |
-                       __vcmpeq4(x, 0x54545454u);
-    if ((m & bytes) != bytes) pure = false;
-    uint32_t c = ((x >> 1) ^ (x >> 2)) & 0x03030303u & bytes;
-    c |= c >> 6;
-    c |= c >> 12;
-    return c & 0xFFu;
+    const uint32_t c = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
+    const uint32_t sel = (c & 0x3u) | ((c >> 4) & 0x30u) | ((c >> 8) & 0x300u) | ((c >> 12) & 0x3000u);
+    if (((__byte_perm(0x54474341u, 0u, sel) ^ x) & bytes) != 0) pure = false;
+    uint32_t cm = c & bytes;
+    cm |= cm >> 6;
+    cm |= cm >> 12;
+    return cm & 0xFFu;
 }
 
 // Writes "<n><op>" at p, returns its length.
