@@ -23,7 +23,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <unordered_map>
 #include <vector>
 
 #include "pipeline.cuh"
