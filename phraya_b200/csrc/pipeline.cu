@@ -17,7 +17,7 @@
 #include <cub/device/device_select.cuh>
 #include <cub/device/device_run_length_encode.cuh>
 #include <cub/device/device_radix_sort.cuh>
-#include <cub/iterator/counting_input_iterator.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cub/device/device_segmented_sort.cuh>
 
 #include <algorithm>
@@ -1267,7 +1267,7 @@ static phr_status detect_repeats(Ctx* ctx, phr_index* idx, const uint8_t* target
         DeviceArena& A = ctx->pipe;
         A.reset();
         size_t tb = 0;
-        cub::CountingInputIterator<uint32_t> it(0);
+        thrust::counting_iterator<uint32_t> it(0);
         cub::DeviceSelect::Flagged(nullptr, tb, it, static_cast<const uint8_t*>(nullptr),
                                    static_cast<uint32_t*>(nullptr), static_cast<int*>(nullptr),
                                    static_cast<int>(chunk), st);
@@ -1286,7 +1286,7 @@ static phr_status detect_repeats(Ctx* ctx, phr_index* idx, const uint8_t* target
                 repeat_candidate_kernel<<<blocks_for(cnt, 256), 256, 0, st>>>(idx->d_target, base, cnt, n, flag);
             }
             size_t t2 = tb;
-            cub::DeviceSelect::Flagged(tmp, t2, cub::CountingInputIterator<uint32_t>(static_cast<uint32_t>(base)),
+            cub::DeviceSelect::Flagged(tmp, t2, thrust::counting_iterator<uint32_t>(static_cast<uint32_t>(base)),
                                        flag, cand, d_cnt, static_cast<int>(cnt), st);
             int hc = 0;
             PHR_CUDA_TRY(ctx, cudaMemcpyAsync(&hc, d_cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
