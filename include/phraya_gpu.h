@@ -269,9 +269,11 @@ typedef struct {
 /*
  * TargetContext::build (phraya-align/src/executor.rs:431-449): uploads the target
  * bytes, builds the minimizer index (build_minimizer_index, seeding.rs:31-37) and the
- * occurrence cap (seed_occurrence_cap(index, 256), seeding.rs:94-102) on the device.
- * `sketch` may be NULL: the target is then sketched with the library's sketcher at the
- * alphabet's default k/w (DNA 21/11 canonical, protein 6/5 plain).
+ * occurrence cap (seed_occurrence_cap(index, 256), seeding.rs:94-102) on the device, and
+ * finds the target's tandem-repeat regions (detect_tandem_repeats, phraya-core/src/
+ * lib.rs:79-135). `sketch` may be NULL: the target is then sketched with the library's
+ * sketcher at the alphabet's default k/w (DNA 21/11 canonical, protein 6/5 plain).
+ * Sketches of up to 2^31 - 16 minimizers.
  */
 phr_status phr_index_create(phr_ctx* ctx, const uint8_t* target, uint64_t target_len,
                             const phr_sketch* sketch, phr_alphabet alphabet, phr_index** out);
