@@ -201,6 +201,38 @@ def diverse_dna(n, seed):
     return bytes(out)
 
 
+AMINO = b"ACDEFGHIKLMNPQRSTVWY"
+
+
+def diverse_protein(n, seed):
+    """diverse_protein of phraya-align/src/executor.rs:1949-1960 (tests module)."""
+    x = seed & M64
+    out = bytearray()
+    for _ in range(n):
+        x = (x * LCG_A + LCG_C) & M64
+        out.append(AMINO[(x >> 33) % 20])
+    return bytes(out)
+
+
+def protein_wfa_myers_cases():
+    """The 20 query/target pairs of protein_wfa_myers_edit_distance_agree
+    (executor.rs:2001-2027): query diverse_protein(120, 97 s + 1), target = query with
+    substitutions at (s % 5) * 15 % of positions drawn from its own LCG."""
+    cases = []
+    for seed in range(20):
+        q = diverse_protein(120, seed * 97 + 1)
+        t = bytearray(q)
+        rate = seed % 5
+        x = (seed + 12345) & M64
+        for i in range(len(t)):
+            x = (x * LCG_A + LCG_C) & M64
+            if (x >> 40) % 100 < rate * 15:
+                x = (x * LCG_A + 1) & M64
+                t[i] = AMINO[(x >> 33) % 20]
+        cases.append((q, bytes(t)))
+    return cases
+
+
 # ---------------------------------------------------------------------------
 # Independent checkers
 # ---------------------------------------------------------------------------

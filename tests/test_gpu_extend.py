@@ -200,3 +200,14 @@ def test_tune_keys_validated(eng):
     before = eng.get_tune("myers_band_base")
     eng.set_tune("myers_band_base", before)
     assert eng.get_tune("myers_band_base") == before
+
+
+@pytest.mark.parametrize("engine", ENGINES, ids=[NAMES[e] for e in ENGINES])
+def test_protein_pairs_bit_exact(eng, engine):
+    """protein_wfa_myers_edit_distance_agree (executor.rs:2001-2027): protein bytes run the
+    byte path of every engine, bit-exact with the oracle; WFA and Myers agree on ed."""
+    pairs = R.protein_wfa_myers_cases()
+    g = compare(eng, engine, pairs)
+    if engine in (A.ENGINE_WFA_LINEAR, A.ENGINE_MYERS_FIT):
+        other = compare(eng, A.ENGINE_MYERS_FIT if engine == A.ENGINE_WFA_LINEAR else A.ENGINE_WFA_LINEAR, pairs)
+        assert [x[2] for x in g] == [x[2] for x in other]

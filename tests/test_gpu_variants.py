@@ -219,3 +219,13 @@ def test_coverage_track_parity(eng, mode):
     assert np.array_equal(got, exp)
     assert got.any() == (mode == A.COVERAGE_DEPTH)
     track.close()
+
+
+def test_protein_alignment_never_reverse(eng):
+    # protein_alignment_never_attempts_reverse_strand (executor.rs:1965-1995)
+    target = R.diverse_protein(300, 11)
+    region = bytearray(target[100:200])
+    region[50] = ord("C") if region[50] == ord("A") else ord("A")
+    off, var, cov, al = compare_variants(eng, target, [bytes(region)], A.SENSITIVE, A.GAP_AFFINE,
+                                         alphabet=A.ALPHABET_PROTEIN)
+    assert len(var) >= 1 and set(var["strand"].tolist()) == {0}

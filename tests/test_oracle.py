@@ -286,3 +286,29 @@ def test_align_read_stored_empty_sketch_is_no_seed():
     e = (__import__("numpy").zeros(0, "u8"), __import__("numpy").zeros(0, "u4"))
     (res,), st = tg.align_reads([target[50:150]], stored=[e])
     assert res[0] == A.OUT_NO_SEED and res[1] == 0
+
+
+def test_protein_wfa_and_myers_agree():
+    # protein_wfa_myers_edit_distance_agree (phraya-align/src/executor.rs:2001-2027):
+    # both engines compare raw bytes, so their distances agree on protein too
+    for q, t in R.protein_wfa_myers_cases():
+        w = O.wfa_extend(q, t)
+        m = O.myers_extend(q, t)
+        assert w[0] == 0 and m[0] == 0
+        assert w[2] == m[2], (q, t, w, m)
+
+
+def test_protein_alignment_never_reverse():
+    # protein_alignment_never_attempts_reverse_strand (executor.rs:1965-1995): a protein
+    # read with one substitution against its source region aligns forward, and its
+    # variant observations say so
+    target = R.diverse_protein(300, 11)
+    region = bytearray(target[100:200])
+    region[50] = ord("C") if region[50] == ord("A") else ord("A")
+    tg = O.Target(target, A.ALPHABET_PROTEIN)
+    from phraya_b200.batch import PackedReads
+    packed = PackedReads([bytes(region)])
+    rr, aln, cig, _ = tg.align_packed(packed, A.SENSITIVE, A.GAP_AFFINE, nthreads=1)
+    assert rr[0]["has_result"] == 1 and rr[0]["reverse"] == 0
+    off, var, cov, al = tg.variants_packed(packed, rr, aln, cig, A.SENSITIVE)
+    assert len(var) >= 1 and set(var["strand"].tolist()) == {0}
