@@ -71,6 +71,8 @@ def lib():
         L.orc_variants.argtypes = [C.c_void_p, C.POINTER(A.ReadBatch), C.POINTER(A.ReadResultArena),
                                    C.POINTER(A.AlignConfig), C.POINTER(A.VariantConfig),
                                    C.POINTER(A.VariantArena)]
+        L.orc_anchors.restype = C.c_uint64
+        L.orc_anchors.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p]
         L.orc_coverage_merge.restype = None
         L.orc_coverage_merge.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int32, C.c_void_p]
         _lib = L
@@ -217,6 +219,14 @@ def tandem_repeats(seq):
     n = int(lib().orc_tandem_repeats(seq, len(seq), st.ctypes.data, en.ctypes.data, cap))
     assert n <= cap
     return [(int(a), int(b)) for a, b in zip(st[:n], en[:n])]
+
+
+def anchors(chain_target_starts, strategy):
+    """anchors_from_chains: target positions of the anchors (query position 0 each)."""
+    st = np.ascontiguousarray(chain_target_starts, dtype=np.uint32)
+    out = np.zeros(max(len(st), 1), dtype=np.uint32)
+    n = int(lib().orc_anchors(st.ctypes.data if len(st) else None, len(st), strategy, out.ctypes.data))
+    return out[:n].tolist()
 
 
 def coverage_merge(aln, tlen, depth=False, track=None):

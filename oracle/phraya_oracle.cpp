@@ -1109,17 +1109,27 @@ struct Target {
 
 size_t chain_cap(int strategy) { return strategy == PHR_FAST ? 1 : strategy == PHR_BALANCED ? 2 : 50; }
 
-// extend_chains (executor.rs:528-567) with anchors_from_chains (:347-362) and
-// extend_anchor (:379-404). Returns false for None.
-bool extend_chains(const Target& tg, const phr_align_config& cfg, const uint8_t* q, size_t qlen,
-                   const std::vector<ChainT>& chains, Scored* out) {
+// anchors_from_chains (executor.rs:347-362): the target starts of the first K chains
+// (K = chain_cap), or the origin when there is no chain. Only target positions vary (the
+// query position of every anchor is 0).
+std::vector<uint32_t> anchors_from_chains(const std::vector<uint32_t>& chain_starts, int strategy) {
     std::vector<uint32_t> anchors;
-    if (chains.empty()) {
+    if (chain_starts.empty()) {
         anchors.push_back(0);
     } else {
-        size_t K = std::min(chain_cap(cfg.strategy), chains.size());
-        for (size_t i = 0; i < K; ++i) anchors.push_back(chains[i].target_start());
+        const size_t K = std::min(chain_cap(strategy), chain_starts.size());
+        for (size_t i = 0; i < K; ++i) anchors.push_back(chain_starts[i]);
     }
+    return anchors;
+}
+
+// extend_chains (executor.rs:528-567) with anchors_from_chains and extend_anchor
+// (:379-404). Returns false for None.
+bool extend_chains(const Target& tg, const phr_align_config& cfg, const uint8_t* q, size_t qlen,
+                   const std::vector<ChainT>& chains, Scored* out) {
+    std::vector<uint32_t> starts;
+    for (const ChainT& c : chains) starts.push_back(c.target_start());
+    const std::vector<uint32_t> anchors = anchors_from_chains(starts, cfg.strategy);
     std::vector<Aln> alns;
     const phr_affine_costs def_costs{2, 4, 1};
     for (uint32_t a : anchors) {
@@ -1693,6 +1703,13 @@ void orc_coverage_merge(const phr_alignment* aln, uint64_t n, uint64_t tlen, int
             track[p] += depth ? c : ((c + 2) / 5) * 5;
         }
     }
+}
+
+// anchors_from_chains over chain target starts (in chain order); returns the anchor count.
+uint64_t orc_anchors(const uint32_t* chain_starts, uint64_t n, int32_t strategy, uint32_t* out) {
+    const std::vector<uint32_t> a = anchors_from_chains(std::vector<uint32_t>(chain_starts, chain_starts + n), strategy);
+    for (size_t i = 0; i < a.size(); ++i) out[i] = a[i];
+    return a.size();
 }
 
 }  // extern "C"

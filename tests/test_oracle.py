@@ -312,3 +312,13 @@ def test_protein_alignment_never_reverse():
     assert rr[0]["has_result"] == 1 and rr[0]["reverse"] == 0
     off, var, cov, al = tg.variants_packed(packed, rr, aln, cig, A.SENSITIVE)
     assert len(var) >= 1 and set(var["strand"].tolist()) == {0}
+
+
+def test_anchors_from_chains_reference_cases():
+    # executor.rs tests anchors_from_chains_falls_back_to_origin_when_no_chains and
+    # anchors_from_chains_uses_chain_target_start_and_respects_cap (:1170-1239)
+    assert O.anchors([], A.FAST) == [0]
+    chains = [100, 5000, 9000]  # target starts of chains scored 30, 25, 20 (chain order)
+    assert O.anchors(chains, A.FAST) == [100]
+    assert O.anchors(chains, A.BALANCED) == [100, 5000]
+    assert O.anchors(chains, A.SENSITIVE) == [100, 5000, 9000]
