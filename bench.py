@@ -522,7 +522,8 @@ def run_pipeline(eng, dev, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20,
+                    help="timed steps (20 keep the timed region near 0.7 s, several clock samples)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n-a", type=int, default=N_A_DEFAULT)
