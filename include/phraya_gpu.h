@@ -492,6 +492,10 @@ typedef struct {
  * min_repeat_count 3, phraya-core/src/lib.rs:79-135). The coverage track the reference
  * stores per read is each alignment's span with quantize_coverage(1) = 0
  * (executor.rs:1092-1096), i.e. derived from the alignments alone.
+ * `vcfg` may be NULL (the strategy's radius, no hotspots). If the variant arena is too
+ * small the call returns PHR_ERR_CAPACITY with variant_used / coverage_used /
+ * allele_used set to the sizes needed (the read results in `out` are complete); call
+ * again with a larger arena.
  */
 phr_status phr_align_reads_variants(phr_ctx* ctx, const phr_index* idx, const phr_read_batch* reads,
                                     const phr_align_config* cfg, phr_read_result_arena* out,
