@@ -1,0 +1,68 @@
+"""bench.py's host-side pieces that the JSON line depends on, on the CPU: the roofline
+object of each extension kernel (achieved / peak = frac, the bound chosen by the longer
+lower-bound time), the clock sampler's reading of nvidia-smi lines, and the CPU baseline
+(the oracle on a bounded sample, scaled to the job)."""
+import importlib.util
+import os
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="module")
+def sets(bench):
+    return bench.make_workload(2000, 300, seed=0)
+
+
+def test_roofline_fields(bench, sets):
+    set_a, set_b = sets
+    work = {"myers_lane_block_columns": 3.0e6, "myers_lane_redo_pairs": 1,
+            "wfa_affine_cells": 7.0e5, "wfa_affine_lcp_words": 6.0e5,
+            "wfa_linear_cells": 2.4e5, "wfa_linear_lcp_words": 2.6e5}
+    int_peak, hbm_peak = 37.2e12, 6.65e12
+    for name in ("myers_lane", "wfa_affine", "wfa_linear"):
+        r = bench.roofline(name, 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")
+        for key in ("bound", "achieved", "peak", "unit", "frac", "traffic", "kernel", "work", "int_frac", "hbm_frac"):
+            assert key in r, (name, key)
+        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+        # the bound is the resource with the longer lower-bound time
+        assert r["bound"] == ("hbm" if r["hbm_frac"] >= r["int_frac"] else "int")
+        assert r["unit"] == ("GB/s" if r["bound"] == "hbm" else "Tops/s")
+    r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")
+    assert r["traffic"] == pytest.approx(7.59e9 * set_b.n / 100000)
+    assert bench.roofline("pack", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")["bound"] is None
+
+
+def test_clock_sampler_reasons(bench):
+    s = bench.ClockSampler(0)  # parsing only: a stand-in for the nvidia-smi process
+    s.lines = ["0, 1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+               "0, 1900, 1965, 990.0, 0x4, Not Active, Not Active, Not Active, Active",
+               "garbage line"]
+
+    class _P:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    s.proc = _P()
+    c = s.stop()
+    assert c["samples"] == 2 and c["sm_max_mhz"] == 1965.0 and c["sm_mhz"] == pytest.approx(1932.5)
+    assert c["reasons"] == ["sw_power_cap"]
+
+
+def test_cpu_baseline_scales_sample(bench, sets):
+    set_a, set_b = sets
+    b = bench.cpu_baseline(set_a, set_b, 1_000_000, 1_000_000, 2, sample_a=500, sample_b=50)
+    assert b["kind"] == "port" and b["cores"] == 2 and b["unit"] == "pairs/s" and b["value"] > 0
+    assert "500 set-A pairs" in b["sample"]
