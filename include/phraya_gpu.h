@@ -221,8 +221,9 @@ phr_status phr_extend_percall(phr_ctx* ctx, phr_engine engine, const phr_pair_ba
  * All pointers are DEVICE memory owned by the caller: pair i aligns
  * seq[q_off[i] .. +q_len[i]) against seq[t_off[i] .. +t_len[i]); results go to
  * status[i], edit_distance[i], target_consumed[i], cigar_len[i] and the CIGAR text at
- * cigar + i * cigar_stride. `stream` is a cudaStream_t (NULL = default stream); the call
- * returns after the work on it has finished.
+ * cigar + i * cigar_stride. `stream` is a cudaStream_t (NULL = default stream); every
+ * call copies its error flags device -> host on `stream` and synchronises the stream, so
+ * it returns after the work on it has finished.
  * Limits: |q| <= PHR_NOALLOC_MAX_QUERY, |t| <= PHR_NOALLOC_MAX_TARGET (the reference's
  * Myers regime: queries of at most 500 bases against windows of twice that); longer
  * pairs get status PHR_ERR_ARG and the call returns PHR_ERR_ARG. cigar_stride must be at

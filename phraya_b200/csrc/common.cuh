@@ -53,28 +53,48 @@ __host__ __device__ inline uint32_t ndigits(uint32_t v) {
 // is byte (i%4) of word W + i/4 (little endian). Both arenas carry >= 2 words of zero
 // padding after every sequence so a funnel shift may read one word past the end.
 // ---------------------------------------------------------------------------
+// kCoherent: the words are written earlier in the same kernel (a warp stages them and
+// reads them back after __syncwarp), so they are read with coherent ld.global.cg loads;
+// the read-only path (ld.global.nc) is only for arenas no kernel writes while reading.
 struct Seq2 {
     static constexpr int kPerWord = 16;
     static constexpr int kBits = 2;
+    static constexpr bool kCoherent = false;
 };
 struct SeqB {
     static constexpr int kPerWord = 4;
     static constexpr int kBits = 8;
+    static constexpr bool kCoherent = false;
 };
+// Byte mode over words staged by the reading kernel itself.
+struct SeqBc {
+    static constexpr int kPerWord = 4;
+    static constexpr int kBits = 8;
+    static constexpr bool kCoherent = true;
+};
+
+template <class S>
+__device__ __forceinline__ uint32_t seq_word(const uint32_t* p) {
+    if constexpr (S::kCoherent) {
+        return __ldcg(p);
+    } else {
+        return __ldg(p);
+    }
+}
 
 // Returns 32 bits holding symbols [pos, pos + kPerWord) of the sequence at `base`.
 template <class S>
 __device__ __forceinline__ uint32_t load_window(const uint32_t* __restrict__ base, int32_t pos) {
     const uint32_t w = static_cast<uint32_t>(pos) / S::kPerWord;
     const uint32_t sh = (static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits;
-    const uint32_t lo = __ldg(base + w);
-    const uint32_t hi = __ldg(base + w + 1);
+    const uint32_t lo = seq_word<S>(base + w);
+    const uint32_t hi = seq_word<S>(base + w + 1);
     return __funnelshift_r(lo, hi, sh);
 }
 
 template <class S>
 __device__ __forceinline__ uint32_t sym_at(const uint32_t* __restrict__ base, int32_t pos) {
-    const uint32_t w = __ldg(base + static_cast<uint32_t>(pos) / S::kPerWord);
+    const uint32_t w = seq_word<S>(base + static_cast<uint32_t>(pos) / S::kPerWord);
     return (w >> ((static_cast<uint32_t>(pos) % S::kPerWord) * S::kBits)) & ((1u << S::kBits) - 1);
 }
 

@@ -109,13 +109,13 @@ struct QueryBlock<Seq2> {
     }
 };
 
-template <>
-struct QueryBlock<SeqB> {
+template <class S>
+struct QueryBlockBytes {
     uint32_t w[16];
     uint64_t mask;
     __device__ __forceinline__ void load(const uint32_t* q, int qsh, int blk, uint64_t msk) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) w[k] = load_window<SeqB>(q, qsh + blk * 64 + 4 * k);
+        for (int k = 0; k < 16; ++k) w[k] = load_window<S>(q, qsh + blk * 64 + 4 * k);
         mask = msk;
     }
     __device__ __forceinline__ uint64_t eq(uint32_t c) const {
@@ -129,6 +129,11 @@ struct QueryBlock<SeqB> {
         return e & mask;
     }
 };
+
+template <>
+struct QueryBlock<SeqB> : QueryBlockBytes<SeqB> {};
+template <>
+struct QueryBlock<SeqBc> : QueryBlockBytes<SeqBc> {};
 
 template <class S>
 __device__ __forceinline__ const uint32_t* seq_base(const ExtendParams& P, uint64_t word) {
@@ -214,7 +219,7 @@ __device__ void myers_group(const ExtendParams& P, const PairDesc& d, uint32_t p
             const int j0 = s - gl;
             const bool live = blk_act && j0 >= 0 && j0 < n && !stop_r;
             // every lane keeps the group's current target word; only lane 0 reads it
-            if ((s % S::kPerWord) == 0 && s < n && go) tword = __ldg(tb + s / S::kPerWord);
+            if ((s % S::kPerWord) == 0 && s < n && go) tword = seq_word<S>(tb + s / S::kPerWord);
             if (live) {
                 if (gl == 0) {
                     // lane 0: target symbol j0 and the carries entering block 0 of the stripe
@@ -503,7 +508,13 @@ namespace phr {
 namespace {
 
 constexpr int kNoAllocWarps = 128;
+// Control block at the start of the array (zeroed by every call): the error flags word
+// (bit 0: a pair beyond the length limits, bit 1: a pair that did not finish) at byte
+// kNoAllocFlagsByte, read back by the host, and the 64-bit next-pair counter at byte
+// kNoAllocCounterByte.
 constexpr uint64_t kNoAllocCtl = 256;
+constexpr uint64_t kNoAllocFlagsByte = 4;
+constexpr uint64_t kNoAllocCounterByte = 8;
 constexpr uint64_t kNoAllocSlice = (PHR_NOALLOC_SCRATCH_BYTES - kNoAllocCtl) / kNoAllocWarps / 256 * 256;
 constexpr uint64_t kNoAllocHeader = 256;
 constexpr uint64_t kNoAllocStageQ = (PHR_NOALLOC_MAX_QUERY / 4 + 8) * 4;
@@ -542,7 +553,8 @@ __device__ uint32_t noalloc_write_count_op(char* p, uint32_t n, char op) {
 __global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
     const int lane = lane_id();
     const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    uint32_t* ctl = reinterpret_cast<uint32_t*>(A.scratch);  // [0] next pair, [1] error flags
+    uint32_t* flags = reinterpret_cast<uint32_t*>(A.scratch + kNoAllocFlagsByte);
+    unsigned long long* next_pair = reinterpret_cast<unsigned long long*>(A.scratch + kNoAllocCounterByte);
     uint8_t* slice = A.scratch + kNoAllocCtl + w * kNoAllocSlice;
     PairOut* pout = reinterpret_cast<PairOut*>(slice);
     uint64_t* toff = reinterpret_cast<uint64_t*>(slice + 64);
@@ -554,7 +566,7 @@ __global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
     uint8_t* work = slice + kNoAllocWork;
     for (;;) {
         uint64_t i = 0;
-        if (lane == 0) i = atomicAdd(reinterpret_cast<unsigned long long*>(ctl + 2), 1ull);
+        if (lane == 0) i = atomicAdd(next_pair, 1ull);
         i = __shfl_sync(PHR_FULL_MASK, i, 0);
         if (i >= A.n) break;
         const uint32_t ql = A.q_len[i], tl = A.t_len[i];
@@ -565,7 +577,7 @@ __global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
                 A.ed[i] = 0;
                 A.consumed[i] = 0;
                 A.cigar_len[i] = 0;
-                atomicOr(ctl + 1, 1u);
+                atomicOr(flags, 1u);
             }
             continue;
         }
@@ -631,7 +643,8 @@ __global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
         int G = 1;
         const int nb = static_cast<int>((ql + 63) / 64);
         while (G < nb) G <<= 1;
-        myers_group<SeqB>(P, d, 0, lane < G, G, work, 0, true);
+        // the staged words were written by this warp above: coherent loads (SeqBc)
+        myers_group<SeqBc>(P, d, 0, lane < G, G, work, 0, true);
         __syncwarp();
         if (lane == 0) {
             const PairOut o = *pout;
@@ -640,7 +653,7 @@ __global__ void __launch_bounds__(256) myers_noalloc_kernel(NoAllocArgs A) {
             A.ed[i] = ok ? static_cast<uint32_t>(o.ed) : 0;
             A.consumed[i] = ok ? static_cast<uint32_t>(o.t_consumed) : 0;
             A.cigar_len[i] = ok ? o.text_len : 0;
-            if (!ok) atomicOr(ctl + 1, 2u);
+            if (!ok) atomicOr(flags, 2u);
         }
         __syncwarp();
     }
@@ -692,7 +705,7 @@ extern "C" phr_status phr_myers_extend_noalloc(const uint8_t* seq, const uint64_
     phr::myers_noalloc_kernel<<<phr::kNoAllocWarps * 32 / 256, 256, 0, st>>>(A);
     if (cudaGetLastError() != cudaSuccess) return PHR_ERR_CUDA;
     uint32_t flags = 0;
-    if (cudaMemcpyAsync(&flags, scratch + 4, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PHR_ERR_CUDA;
+    if (cudaMemcpyAsync(&flags, scratch + phr::kNoAllocFlagsByte, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PHR_ERR_CUDA;
     if (cudaStreamSynchronize(st) != cudaSuccess) return PHR_ERR_CUDA;
     if (flags & 2u) return PHR_ERR_CUDA;
     if (flags & 1u) return PHR_ERR_ARG;

@@ -30,6 +30,69 @@
 
 namespace {
 
+// Servers raise the release threshold of their device's default memory pool to its
+// maximum (freed memory stays in the pool, so workers growing and shrinking arenas never
+// wait on unmapping while others run). Servers on one device share that setting: the
+// first one saves the caller's threshold and the last one to go restores it.
+struct PoolHold {
+    int servers = 0;
+    cudaMemPool_t pool = nullptr;
+    uint64_t saved = 0;
+};
+std::mutex g_pool_mu;
+PoolHold g_pool_hold[256];
+
+bool pool_hold_acquire(int dev) {
+    if (dev < 0 || dev >= 256) return false;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    PoolHold& h = g_pool_hold[dev];
+    if (h.servers == 0) {
+        cudaMemPool_t pool = nullptr;
+        uint64_t saved = 0;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess ||
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &saved) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        uint64_t keep = UINT64_MAX;
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        h.pool = pool;
+        h.saved = saved;
+    }
+    ++h.servers;
+    return true;
+}
+
+void pool_hold_release(int dev) {
+    if (dev < 0 || dev >= 256) return;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    PoolHold& h = g_pool_hold[dev];
+    if (h.servers <= 0) return;
+    if (--h.servers == 0 && h.pool) {
+        cudaMemPoolSetAttribute(h.pool, cudaMemPoolAttrReleaseThreshold, &h.saved);
+        cudaGetLastError();
+        h.pool = nullptr;
+    }
+}
+
+// Restores the caller's current device when a server call returns.
+struct DeviceRestore {
+    int dev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    }
+    ~DeviceRestore() {
+        if (dev >= 0) cudaSetDevice(dev);
+    }
+};
+
+}  // namespace
+
+namespace {
+
 using Clock = std::chrono::steady_clock;
 
 struct Request {
@@ -85,10 +148,8 @@ struct phr_server {
     uint64_t in_flight = 0;            // submitted, not yet completed
     uint64_t completions = 0;          // batches finished (admission waits on it)
     bool stopping = false;
-    // the device's default memory pool and its release threshold before this server
-    // raised it (restored at destroy)
-    cudaMemPool_t pool = nullptr;
-    uint64_t pool_threshold = 0;
+    // this server holds a reference on its device's memory-pool setting (pool_hold_*)
+    bool pool_held = false;
     bool short_lane = false;
     phr_status fatal = PHR_OK;
     std::string fatal_msg;
@@ -340,19 +401,14 @@ phr_status phr_server_create(phr_ctx* c, const phr_index* idx, const phr_server_
         delete S;
         return PHR_ERR_ARG;
     }
+    DeviceRestore restore_device;
     int prio_low = 0, prio_high = 0;
     cudaSetDevice(c->impl.device);
     cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
     // workers' arenas grow and shrink through the device's default memory pool; keeping
     // freed memory in the pool (no release threshold) spares them unmapping and mapping it
     // again while other workers run
-    if (cudaDeviceGetDefaultMemPool(&S->pool, c->impl.device) == cudaSuccess &&
-        cudaMemPoolGetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    } else {
-        S->pool = nullptr;
-    }
+    S->pool_held = pool_hold_acquire(c->impl.device);
     cudaGetLastError();
     for (uint32_t w = 0; w < S->cfg.n_streams; ++w) {
         auto* W = new phr_server::Worker();
@@ -369,6 +425,7 @@ phr_status phr_server_create(phr_ctx* c, const phr_index* idx, const phr_server_
         if (cudaStreamCreateWithPriority(&W->ctx.stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
             delete W;
             for (auto* x : S->workers) delete x;
+            if (S->pool_held) pool_hold_release(c->impl.device);
             delete S;
             return PHR_ERR_CUDA;
         }
@@ -463,6 +520,7 @@ phr_status phr_server_poll(phr_server* S, phr_server_result* res, uint32_t max_r
 
 phr_status phr_server_destroy(phr_server* S) {
     if (!S) return PHR_ERR_ARG;
+    DeviceRestore restore_device;
     {
         std::unique_lock<std::mutex> lk(S->mu);
         // drain: every submitted request completes before the workers stop
@@ -483,7 +541,7 @@ phr_status phr_server_destroy(phr_server* S) {
         cudaStreamSynchronize(W->ctx.stream);
         delete W;
     }
-    if (S->pool) cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &S->pool_threshold);
+    if (S->pool_held) pool_hold_release(S->owner->device);
     delete S;
     return st;
 }

@@ -5,8 +5,9 @@ example code sharing the GPU with a caching allocator that already holds its mem
 latency-critical loops that must avoid cudaMalloc/cudaFree and their implicit
 synchronisation). Its scratch is one fixed array inside the library, so this test checks
 that it returns exactly what the regular batched entry point (phr_extend_batch with
-PHR_ENGINE_MYERS_FIT) returns, on two calls in a row that reuse that array, and that
-pairs beyond its stated length limits are refused with PHR_ERR_ARG.
+PHR_ENGINE_MYERS_FIT) returns and exactly what the CPU oracle's myers_extend returns, on
+two calls in a row that reuse that array, and that pairs beyond its stated length limits
+are refused with PHR_ERR_ARG.
 
 The file name sorts last so a run that stops at the first failure has run every other
 test before this one.
@@ -16,6 +17,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle as O
 from phraya_b200 import _abi as A
 from phraya_b200 import api as P
 from phraya_b200 import datagen as D
@@ -84,11 +86,15 @@ def test_noalloc_matches_batched_entry_point_twice():
         packed = PackedPairs(make_pairs(seed))
         aln, cig = eng.extend_packed(A.ENGINE_MYERS_FIT, packed)
         ref = [(r[0], r[1], r[2], r[6] - r[5]) for r in P.unpack(aln, cig)]
+        oa, oc = O.extend_packed(A.ENGINE_MYERS_FIT, packed, (2, 4, 1))
+        orc = [(r[0], r[1], r[2], r[6] - r[5]) for r in P.unpack(oa, oc)]
         d, out = device_batch(torch, packed)
         assert run_noalloc(L, torch, d, out, packed.n) == A.PHR_OK
         got = results(out, packed.n)
         bad = [i for i in range(packed.n) if got[i] != ref[i]]
         assert not bad, (len(bad), got[bad[0]], ref[bad[0]])
+        bad = [i for i in range(packed.n) if got[i] != orc[i]]
+        assert not bad, (len(bad), got[bad[0]], orc[bad[0]])
     eng.close()
 
 
