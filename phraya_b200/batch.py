@@ -112,6 +112,25 @@ class PackedReads:
             self.s_values = np.array(vals + [0], dtype=np.uint64)
             self.s_positions = np.array(poss + [0], dtype=np.uint32)
 
+    @classmethod
+    def from_arrays(cls, seq, off, lens):
+        """Wraps an existing arena (uint8) with per-read offsets (uint64) and lengths (uint32)."""
+        self = cls.__new__(cls)
+        self.seq = np.ascontiguousarray(seq, dtype=np.uint8) if len(seq) else np.zeros(1, np.uint8)
+        self.off = np.ascontiguousarray(off, dtype=np.uint64)
+        self.len = np.ascontiguousarray(lens, dtype=np.uint32)
+        self.n = len(self.len)
+        self.has_stored = None
+        return self
+
+    def read(self, i):
+        o = int(self.off[i])
+        return bytes(self.seq[o:o + int(self.len[i])])
+
+    def subset(self, idx):
+        """A new batch holding reads `idx` (in that order)."""
+        return PackedReads([self.read(int(i)) for i in idx])
+
     def batch(self):
         b = A.ReadBatch()
         b.n_reads = self.n
