@@ -564,9 +564,11 @@ typedef struct {
 } phr_server_result;
 
 /* While a server exists, the device's default CUDA memory pool keeps memory freed to it
- * (release threshold raised to the maximum; the previous value is restored by
- * phr_server_destroy), so the workers' arenas can grow again without the driver mapping
- * memory while other workers' kernels run. */
+ * (release threshold raised to the maximum), so the workers' arenas can grow again
+ * without the driver mapping memory while other workers' kernels run. Servers on one
+ * device share that setting: the threshold in force before the first of them was
+ * created is restored when the last of them is destroyed. Create and destroy leave the
+ * caller's current device unchanged. */
 phr_status phr_server_create(phr_ctx* ctx, const phr_index* idx, const phr_server_config* cfg,
                              phr_server** out);
 /* Enqueues one read (bytes copied); returns its request id in *request_id. */

@@ -11,7 +11,10 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libphraya_b200.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["engine.cu", "myers.cu", "myers_lane.cu", "wfa.cu", "api.cu", "pipeline.cu", "server.cu"]
+# the CUDA translation units of the library, one per line; the Rust crate's build.rs
+# (rust/phraya-gpu-sys) reads the same list
+with open(os.path.join(CSRC, "SOURCES")) as _fh:
+    SOURCES = [ln.strip() for ln in _fh if ln.strip() and not ln.startswith("#")]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
