@@ -1,0 +1,70 @@
+"""Failure paths of the C ABI that are made on the host: a scratch budget too small for
+one pair ends the call with PHR_ERR_OOM and a message, and the context stays usable;
+bad arguments are refused with PHR_ERR_ARG before any work; a result arena too small
+for the CIGAR text gives PHR_ERR_CAPACITY. No kernel is made to fail."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+from phraya_b200 import _abi as A
+from phraya_b200 import api as P
+from phraya_b200 import datagen as D
+from phraya_b200.batch import PackedPairs
+
+pytestmark = pytest.mark.gpu
+
+
+def divergent_pair(n, seed):
+    rng = np.random.default_rng(seed)
+    q = bytes(rng.choice(list(b"ACGT"), n).tolist())
+    t = bytes(rng.choice(list(b"ACGT"), n).tolist())
+    return q, t
+
+
+def test_workspace_too_small_is_oom_and_context_survives():
+    small = D.extension_pairs(64, 100, 300, 0.05, seed=31)
+    with P.Engine(0, workspace_bytes=1 << 16) as eng:
+        with pytest.raises(P.EngineError) as ei:
+            eng.extend(A.ENGINE_WFA_LINEAR, [divergent_pair(20000, 1)])
+        assert ei.value.status == A.PHR_ERR_OOM
+        assert "scratch" in str(ei.value)
+        # the same context still aligns pairs that fit its budget
+        ga, gc = eng.extend_packed(A.ENGINE_WFA_AFFINE, small, P.AffineCosts(4, 6, 2))
+        oa, oc = O.extend_packed(A.ENGINE_WFA_AFFINE, small, (4, 6, 2))
+        assert P.unpack(ga, gc) == P.unpack(oa, oc)
+
+
+def test_bad_arguments_are_refused():
+    with P.Engine(0) as eng:
+        L = eng._lib
+        p = PackedPairs([(b"ACGT", b"ACGT")])
+        aln = np.zeros(1, dtype=P.ALN_DTYPE)
+        cig = np.zeros(16, dtype=np.uint8)
+        arena = A.ResultArena(aln.ctypes.data, cig.ctypes.data, 16, 0)
+        b = p.batch()
+        costs = A.AffineCosts(2, 4, 1)
+        assert L.phr_extend_batch(eng.handle, 9, C.byref(b), costs, C.byref(arena)) == A.PHR_ERR_ARG
+        assert L.phr_extend_batch(eng.handle, A.ENGINE_MYERS_FIT, None, costs, C.byref(arena)) == A.PHR_ERR_ARG
+        assert L.phr_extend_batch(eng.handle, A.ENGINE_MYERS_FIT, C.byref(b), costs, None) == A.PHR_ERR_ARG
+        # a pair whose sequence runs past the arena end
+        bad = p.batch()
+        bad.seq_bytes = 6
+        assert L.phr_extend_batch(eng.handle, A.ENGINE_MYERS_FIT, C.byref(bad), costs,
+                                  C.byref(arena)) == A.PHR_ERR_ARG
+        # the context still works
+        assert L.phr_extend_batch(eng.handle, A.ENGINE_MYERS_FIT, C.byref(b), costs, C.byref(arena)) == A.PHR_OK
+        assert bytes(cig[:arena.cigar_used]) == b"4M"
+
+
+def test_cigar_arena_too_small_is_capacity():
+    p = D.extension_pairs(50, 100, 300, 0.05, seed=32)
+    with P.Engine(0) as eng:
+        L = eng._lib
+        aln = np.zeros(p.n, dtype=P.ALN_DTYPE)
+        cig = np.zeros(8, dtype=np.uint8)
+        arena = A.ResultArena(aln.ctypes.data, cig.ctypes.data, 8, 0)
+        b = p.batch()
+        st = L.phr_extend_batch(eng.handle, A.ENGINE_WFA_LINEAR, C.byref(b), A.AffineCosts(2, 4, 1), C.byref(arena))
+        assert st == A.PHR_ERR_CAPACITY
