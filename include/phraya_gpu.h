@@ -33,7 +33,8 @@ typedef enum {
     PHR_INVALID_INPUT = 1,     /* WfaError::InvalidInput (seed beyond sequence end)   */
     PHR_ALIGNMENT_FAILED = 2,  /* WfaError::AlignmentFailed (search exhausted)         */
     PHR_ERR_OOM = 3,           /* device allocation failed / not enough free HBM      */
-    PHR_ERR_TIMEOUT = 4,       /* a bounded device wait gave up                        */
+    /* 4 is unused: no entry point waits on the device with a time limit (no kernel spins
+     * on a flag; the persistent kernels take work from an atomic queue head). */
     PHR_ERR_CUDA = 5,          /* CUDA runtime error or no usable device               */
     PHR_ERR_ARG = 6,           /* bad argument: NULL pointer, size over a stated limit */
     PHR_ERR_CAPACITY = 7,      /* caller-supplied output arena too small               */
@@ -139,6 +140,10 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *                                        kernels (1..4)
  *   "host_chunks"                        chunks a host batch of more than 128 MiB of sequence
  *                                        is copied and aligned in, overlapped (2..32, default 4)
+ *   "myers_lane_ckpt"                    banded Myers (global 2-bit pairs): 1 = keep the band's
+ *                                        state every 4th column and recompute 4 columns at a
+ *                                        time in shared memory for the traceback (default),
+ *                                        0 = store every column's records
  * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune
  * file (written by the autotuner); unknown keys and bad values there are ignored. */
 phr_status phr_ctx_set_tune(phr_ctx* ctx, const char* key, int64_t value);
@@ -283,8 +288,15 @@ phr_status phr_index_get_info(const phr_index* idx, phr_index_info* info);
 
 /*
  * The library's minimizer sketcher: canonical (DNA) or plain (protein) (k, w)
- * minimizers of every sequence in the batch. Stands in for simd-minimizers at
- * phraya-core/src/types.rs:1848-1869 (the same function the oracle restates).
+ * minimizers of every sequence in the batch, k in 1..32. Restates simd-minimizers
+ * 2.3.1 as phraya-core/src/types.rs:1848-1869 calls it (over packed-seq's AsciiSeq):
+ * characters as 2-bit codes (b >> 1) & 3; 32-bit ntHash order hashes (canonical: the
+ * smaller of the forward and reverse-complement hashes); per window of w k-mers the
+ * leftmost minimum, or, for canonical minimizers, the rightmost one in windows whose
+ * w + k - 1 characters hold no more T/G than A/C; each selected k-mer once per run of
+ * windows; value = the 2-bit k-mer, first character lowest (DNA: the smaller of the
+ * k-mer and its reverse complement). The crate itself is not available to check
+ * against, so sketches are not guaranteed identical to its.
  * Sequence i is seq[off[i] .. off[i]+len[i]). Output: sequence i's minimizers at
  * values/positions[out_off[i] .. out_off[i] + out_n[i]); capacity per sequence is
  * max(len[i] - k + 1, 0) entries, so out_off must leave that much room.

@@ -12,10 +12,11 @@
 // tests/ (see tests/golden/known_answers.json).
 //
 // The minimizer sketcher is the one exception: phraya uses the third-party crate
-// simd-minimizers 2.3 (phraya-core/Cargo.toml; call site phraya-core/src/types.rs:
-// 1848-1869), which is not available here. `orc_sketch` is this project's documented
-// replacement scheme, shared bit-for-bit with the CUDA sketcher; parity at the
-// sketching boundary is therefore unpinned.
+// simd-minimizers 2.3.1 (phraya-core/Cargo.toml; version named in
+// docs/adr/0013-protein-space-alphabet-support.md:31; call site phraya-core/src/types.rs:
+// 1848-1869), whose source is not in the reference tree. `sketch_seq` restates its
+// published algorithm (see the comment there); no reference test pins minimizer values
+// or positions, so parity at the sketching boundary is unpinned.
 
 #include <emmintrin.h>
 
@@ -853,52 +854,76 @@ Aln extend_one(phr_engine engine, const uint8_t* q, int32_t qlen, const uint8_t*
 }
 
 // ---------------------------------------------------------------------------
-// Minimizer sketcher (this project's documented scheme; see file header).
-//   code(b) = (b >> 1) & 3  (A=0, C=1, T=2, G=3 for either case; any other byte maps
-//   to one of the four codes). DNA: the k-mer's forward value F packs codes first-base
-//   most significant; its reverse complement R packs (code ^ 2) of the bases in
-//   reverse order; the canonical value is min(F, R). Protein: F packs the k raw bytes
-//   (8 bits each, first byte most significant) and is used as-is. The order key is
-//   mix64(value) (the SplitMix64 finalizer). Every window of w consecutive k-mers
-//   selects its leftmost minimum-key k-mer; consecutive windows selecting the same
-//   k-mer emit it once. Output pairs are (mix64(value), k-mer start position).
+// Minimizer sketcher: simd-minimizers' random minimizers restated from their published
+// descriptions (the crate is not in the reference tree).
+//   * Characters: packed-seq's AsciiSeq view, which the call site uses for DNA and
+//     protein alike (types.rs:1849-1862): 2 bits per character, code(b) = (b >> 1) & 3,
+//     i.e. A = 0, C = 1, T = 2, G = 3 for either case; the complement is code ^ 2.
+//   * Order hash: ntHash (Mohamadi et al., Bioinformatics 2016; "ntHash rolling hashes",
+//     README.md:185) in 32 bits, the lane width of the SIMD sketcher (Groot Koerkamp &
+//     Martayan, SEA 2025): h_fw = XOR_i rotl(seed[x_i], k-1-i), h_rc = XOR_i
+//     rotl(seed[comp(x_i)], i), over the four published ntHash base seeds (low 32 bits).
+//     Canonical (DNA): min(h_fw, h_rc), ntHash's canonical hash; plain (protein): h_fw.
+//   * Window: w consecutive k-mers (l = w + k - 1 characters). Plain minimizers take the
+//     leftmost minimum hash. Canonical minimizers (odd l, README.md:190) orient each
+//     window by its characters: a window with more T/G than A/C (codes 2, 3 against
+//     0, 1) is forward and takes the leftmost minimum, otherwise the rightmost, so a
+//     sequence and its reverse complement select the same k-mers (SEA 2025).
+//   * Output: each selected k-mer once per run of windows selecting it (the crate's
+//     minimizer positions), paired with its value (`pos_and_values_u64`): the 2-bit
+//     k-mer, first character in the low bits; canonical: min(forward, reverse
+//     complement) (docs/adr/0013-protein-space-alphabet-support.md:20-21).
 // ---------------------------------------------------------------------------
-inline uint64_t mix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
+constexpr uint32_t kNtSeed[4] = {
+    static_cast<uint32_t>(0x3c8bfbb395c60474ull),  // A (code 0)
+    static_cast<uint32_t>(0x3193c18562a02b4cull),  // C (code 1)
+    static_cast<uint32_t>(0x295549f54be24456ull),  // T (code 2)
+    static_cast<uint32_t>(0x20323ed082572324ull),  // G (code 3)
+};
+
+inline uint32_t rotl32(uint32_t x, int r) {
+    r &= 31;
+    return r ? (x << r) | (x >> (32 - r)) : x;
 }
 
 void sketch_seq(const uint8_t* s, int64_t len, int k, int w, int alphabet,
                 std::vector<std::pair<uint64_t, uint32_t>>* out) {
     out->clear();
-    if (k <= 0 || w <= 0 || len < k) return;
+    if (k <= 0 || w <= 0 || k > 32 || len < k) return;
+    const bool canonical = alphabet == PHR_ALPHABET_DNA;
     const int64_t nk = len - k + 1;
-    std::vector<uint64_t> key(static_cast<size_t>(nk));
-    if (alphabet == PHR_ALPHABET_DNA) {
-        const uint64_t mask = (k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1);
-        uint64_t f = 0, r = 0;
-        for (int64_t i = 0; i < len; ++i) {
-            uint64_t c = (s[i] >> 1) & 3;
-            f = ((f << 2) | c) & mask;
-            r = (r >> 2) | ((c ^ 2ull) << (2 * (k - 1)));
-            if (i >= k - 1) key[static_cast<size_t>(i - k + 1)] = mix64(f < r ? f : r);
+    std::vector<uint32_t> hash(static_cast<size_t>(nk));
+    std::vector<uint64_t> value(static_cast<size_t>(nk));
+    for (int64_t p = 0; p < nk; ++p) {
+        uint32_t hf = 0, hr = 0;
+        uint64_t vf = 0, vr = 0;
+        for (int i = 0; i < k; ++i) {
+            const uint32_t c = (s[p + i] >> 1) & 3;
+            hf ^= rotl32(kNtSeed[c], k - 1 - i);
+            hr ^= rotl32(kNtSeed[c ^ 2], i);
+            vf |= static_cast<uint64_t>(c) << (2 * i);
+            vr |= static_cast<uint64_t>(c ^ 2) << (2 * (k - 1 - i));
         }
-    } else {
-        for (int64_t p = 0; p < nk; ++p) {
-            uint64_t f = 0;
-            for (int j = 0; j < k; ++j) f = (f << 8) | s[p + j];
-            key[static_cast<size_t>(p)] = mix64(f);
-        }
+        hash[static_cast<size_t>(p)] = canonical ? std::min(hf, hr) : hf;
+        value[static_cast<size_t>(p)] = canonical ? std::min(vf, vr) : vf;
     }
     if (nk < w) return;
+    const int64_t l = w + k - 1;
     int64_t last = -1;
-    for (int64_t wstart = 0; wstart + w <= nk; ++wstart) {
-        int64_t best = wstart;
-        for (int64_t p = wstart + 1; p < wstart + w; ++p)
-            if (key[static_cast<size_t>(p)] < key[static_cast<size_t>(best)]) best = p;
+    for (int64_t ws = 0; ws + w <= nk; ++ws) {
+        bool forward = true;
+        if (canonical) {
+            int64_t tg = 0;
+            for (int64_t i = ws; i < ws + l; ++i) tg += ((s[i] >> 1) & 2) ? 1 : 0;
+            forward = 2 * tg > l;
+        }
+        int64_t best = ws;
+        for (int64_t p = ws + 1; p < ws + w; ++p) {
+            const uint32_t a = hash[static_cast<size_t>(p)], b = hash[static_cast<size_t>(best)];
+            if (a < b || (!forward && a == b)) best = p;
+        }
         if (best != last) {
-            out->push_back({key[static_cast<size_t>(best)], static_cast<uint32_t>(best)});
+            out->push_back({value[static_cast<size_t>(best)], static_cast<uint32_t>(best)});
             last = best;
         }
     }

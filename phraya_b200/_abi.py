@@ -9,7 +9,6 @@ PHR_OK = 0
 PHR_INVALID_INPUT = 1
 PHR_ALIGNMENT_FAILED = 2
 PHR_ERR_OOM = 3
-PHR_ERR_TIMEOUT = 4
 PHR_ERR_CUDA = 5
 PHR_ERR_ARG = 6
 PHR_ERR_CAPACITY = 7

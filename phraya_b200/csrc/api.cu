@@ -320,7 +320,6 @@ const char* phr_status_string(phr_status s) {
         case PHR_INVALID_INPUT: return "invalid input (seed beyond sequence end)";
         case PHR_ALIGNMENT_FAILED: return "alignment failed (search exhausted)";
         case PHR_ERR_OOM: return "out of device memory";
-        case PHR_ERR_TIMEOUT: return "device wait timed out";
         case PHR_ERR_CUDA: return "CUDA error";
         case PHR_ERR_ARG: return "bad argument";
         case PHR_ERR_CAPACITY: return "output arena too small";
@@ -383,6 +382,7 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "max_blocks_per_sm")) return &t.max_blocks_per_sm;
     if (!std::strcmp(key, "wfa_long_min")) return &t.wfa_long_min;
     if (!std::strcmp(key, "host_chunks")) return &t.host_chunks;
+    if (!std::strcmp(key, "myers_lane_ckpt")) return &t.myers_lane_ckpt;
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
@@ -396,6 +396,7 @@ bool tune_valid(const char* key, int64_t v) {
     if (!std::strcmp(key, "max_blocks_per_sm")) return v >= 1 && v <= 4;
     if (!std::strcmp(key, "wfa_long_min")) return v >= 0 && v <= INT32_MAX;
     if (!std::strcmp(key, "host_chunks")) return v >= 2 && v <= 32;
+    if (!std::strcmp(key, "myers_lane_ckpt")) return v == 0 || v == 1;
     return false;
 }
 }  // namespace

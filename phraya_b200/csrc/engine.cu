@@ -387,6 +387,7 @@ struct TaskBuild {
     unsigned int* need_hist;      // 64 buckets by bit length of the need
     int32_t big_min;              // linear WFA pairs for the CTA-per-pair kernel (not in the
     uint32_t big_smem;            // main pass, so not in its slot statistics)
+    int32_t lane_ckpt;            // lane kernel mode (its scratch need)
 };
 
 __device__ __forceinline__ int key_group(uint32_t k) { return 1 << ((k >> 28) & 7); }
@@ -450,7 +451,7 @@ __global__ void task_fill_kernel(TaskBuild T) {
             ++cnt;
         }
         if (T.engine != PHR_ENGINE_MYERS_FIT && T.engine != PHR_ENGINE_MYERS_GLOBAL) need = region * per;
-        if (lane_task && cnt) need = lane_task_need(n_max, m_max, lane_slots(dmin, dmax, (m_max + 63) >> 6));
+        if (lane_task && cnt) need = lane_task_need(n_max, m_max, lane_slots(dmin, dmax, (m_max + 63) >> 6), T.lane_ckpt);
         const uint32_t t = T.tidx[p];
         T.task_first[t] = static_cast<uint32_t>(p);
         T.task_count[t] = static_cast<uint8_t>(cnt);
@@ -751,7 +752,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     PHR_CUDA_TRY(ctx, cudaMemsetAsync(need_hist, 0, 64 * 4, st));
     TaskBuild tbp{keys_s, order, n, head, flag, tidx, task_first, task_count, task_group, cnt, cnt + 4, cnt + 20, desc,
                   engine, ctx->tune.myers_band_base, need_max, task_need, need_hist,
-                  ctx->tune.wfa_big_min, static_cast<uint32_t>(ctx->tune.wfa_big_smem)};
+                  ctx->tune.wfa_big_min, static_cast<uint32_t>(ctx->tune.wfa_big_smem), ctx->tune.myers_lane_ckpt};
     {
         KernelScope ks(ctx, "task_head");
         task_head_kernel<<<blocks_for(n, T), T, 0, st>>>(tbp);
@@ -819,6 +820,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     P.engine = engine;
     P.full_band = 0;
     P.band_base = ctx->tune.myers_band_base;
+    P.lane_ckpt = ctx->tune.myers_lane_ckpt;
     P.costs = costs;
     P.error_flag = cnt + 10;
     P.big_min = ctx->tune.wfa_big_min;
@@ -863,8 +865,9 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         if (!per_task && engine == PHR_ENGINE_MYERS_GLOBAL) {
             // global 2-bit pairs of one lane each (tasks [0, g1)); the warp-group kernel
             // below takes the remaining 2-bit tasks [g1, split)
-            const uint64_t lane_grid = std::min<uint64_t>(grid * warps_per_block / (kLaneThreads / 32),
-                                                          static_cast<uint64_t>(ctx->sm_count) * 2);
+            const uint64_t lane_grid =
+                std::min<uint64_t>(grid * warps_per_block / (kLaneThreads / 32),
+                                   static_cast<uint64_t>(ctx->sm_count) * myers_lane_blocks_per_sm(P.lane_ckpt));
             PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 26, 0, 4, st));
             P.tasks.range = cnt + 28;
             P.queue_head = cnt + 26;

@@ -43,6 +43,8 @@ struct ExtendParams {
     uint32_t big_smem;          // dynamic shared memory of the CTA-per-pair kernel (bytes)
     unsigned long long* work;   // [0] banded Myers block-columns, [1] pairs sent to redo,
                                 // [2] WFA wavefront diagonals, [3] WFA LCP word compares
+    int32_t lane_ckpt;          // banded Myers lane kernel: checkpoints + recomputed segments (1)
+                                // or every column's records (0)
 };
 
 // task_group bit marking a redo task for the CTA-per-pair kernel
@@ -115,11 +117,23 @@ __host__ __device__ __forceinline__ int lane_slots(int dmin, int dmax, int nb) {
     return p < nb ? p : nb;
 }
 
-// Scratch of one lane task: 16-byte {VP, HP} records [column group][slot][lane][column
-// in group], then one reverse-run list of (m_max + n_max + 2) words per lane.
-__host__ __device__ __forceinline__ uint64_t lane_task_need(int n_max, int m_max, int P) {
+// Columns per traceback segment of the checkpointed lane kernel: the forward pass keeps
+// the window's {VP, VN} after every kSegCols-th column, the traceback recomputes one
+// segment of columns at a time into shared memory.
+constexpr int kSegCols = 4;
+
+// Scratch of one lane task, then one reverse-run list of (m_max + n_max + 2) words per
+// lane. Record mode: 16-byte {VP, HP} records [column group][slot][lane][column in
+// group] of every column. Checkpoint mode: 16-byte {VP, VN} states [checkpoint][slot]
+// [lane] after columns kSegCols, 2 kSegCols, ... below n_max.
+__host__ __device__ __forceinline__ uint64_t lane_rec_bytes(int n_max, int P, int ckpt) {
     const uint64_t ng = static_cast<uint64_t>((n_max + kLaneColGroup - 1) / kLaneColGroup);
-    const uint64_t rec = (ng * kLaneColGroup * P * 512 + 255) & ~255ull;
+    const uint64_t nck = n_max > 0 ? static_cast<uint64_t>((n_max - 1) / kSegCols) : 0;
+    return ckpt ? ((nck * P * 512 + 255) & ~255ull) : ((ng * kLaneColGroup * P * 512 + 255) & ~255ull);
+}
+
+__host__ __device__ __forceinline__ uint64_t lane_task_need(int n_max, int m_max, int P, int ckpt = 0) {
+    const uint64_t rec = lane_rec_bytes(n_max, P, ckpt);
     const uint64_t runs = (32ull * static_cast<uint64_t>(m_max + n_max + 2) * 4 + 255) & ~255ull;
     return rec + runs;
 }
@@ -135,6 +149,8 @@ __host__ __device__ __forceinline__ uint64_t myers_full_need(int m, int n) {
 
 void launch_myers(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_myers_lane(const ExtendParams& p, int grid, cudaStream_t st);
+// Resident blocks per SM of the lane kernel in each mode (its shared memory per warp).
+int myers_lane_blocks_per_sm(int ckpt);
 constexpr int kLaneThreads = 256;
 void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st);

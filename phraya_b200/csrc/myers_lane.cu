@@ -129,7 +129,16 @@ __device__ __forceinline__ int lane_blo(const LaneGeom& g, int j) {
     return x > 0 ? (x >> 6) : 0;
 }
 
+// Byte offset of the {VP, VN} state of slot k after column (c + 1) * kSegCols.
 template <int P>
+__device__ __forceinline__ uint64_t ck_off(int c, int k, int lane) {
+    return ((static_cast<uint64_t>(c) * P + k) * 32 + lane) * 16;
+}
+
+// Forward pass of one lane's pair. CK = false: every column's {VP, HP} records go to
+// `rec`; CK = true: only the window's {VP, VN} after every kSegCols-th column below
+// n_max (the traceback recomputes the columns in between).
+template <int P, bool CK>
 __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, const uint32_t* __restrict__ tb, int n,
                                              int nb, const LaneGeom& g, uint64_t* sp, uint8_t* rec) {
     const int lane = lane_id();
@@ -190,10 +199,17 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
             const uint64_t eq = eqp[k * 128];
             const uint64_t ph = k == 0 ? advance_block<true>(vp[0], vn[0], eq, pa, ma)
                                        : advance_block<false>(vp[k], vn[k], eq, pa, ma);
-            *reinterpret_cast<uint4*>(r + k * (512 * kLaneColGroup) + sub * 16) =
-                make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(ph), hi32(ph));
+            if (!CK)
+                *reinterpret_cast<uint4*>(r + k * (512 * kLaneColGroup) + sub * 16) =
+                    make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(ph), hi32(ph));
         }
-        if (sub == kLaneColGroup - 1) r += P * (512 * kLaneColGroup);
+        if (!CK && sub == kLaneColGroup - 1) r += P * (512 * kLaneColGroup);
+        if (CK && (j % kSegCols) == 0 && j < g.n_max) {  // warp-uniform
+            uint8_t* c = rec + ck_off<P>(j / kSegCols - 1, 0, lane);
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                *reinterpret_cast<uint4*>(c + k * 512) = make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(vn[k]), hi32(vn[k]));
+        }
     }
 }
 
@@ -346,11 +362,157 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
     return ok;
 }
 
+// Shared memory of one warp in checkpoint mode: the Peq ring (kLaneMaxSlots + 1 blocks,
+// [block % (P + 1)][base][lane], 64-bit masks) then one segment's {VP, HP} records
+// [column][slot][lane]. The forward pass's Peq ([slot][base][lane]) reuses its start.
+constexpr int kRingBytes = (kLaneMaxSlots + 1) * 4 * 32 * 8;
+constexpr int kCkWarpBytes = kRingBytes + kSegCols * kLaneMaxSlots * 32 * 16;
+
+// Peq of query block b (zero past the query) into ring slot b % (P + 1).
+template <int P>
+__device__ __forceinline__ void ring_fill(uint64_t* ring, const uint32_t* __restrict__ qb, int b, int nb, int lane) {
+    uint64_t e[4] = {0, 0, 0, 0};
+    if (b < nb) {
+        uint32_t qw[4];
+        load_block_words(qb, b, qw);
+        peq_words(qw, e);
+    }
+    uint64_t* r = ring + (b % (P + 1)) * 128 + lane;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) r[c * 32] = e[c];
+}
+
+// Traceback of one lane's pair from (m, n) over segments of kSegCols columns, top
+// segment first. For each segment the warp recomputes its columns from the forward
+// pass's checkpoint (the same window, shifts and block updates, so the same bits), keeps
+// their {VP, HP} records in shared memory, and every lane whose walk is inside the
+// segment moves through it one event at a time (D run, I move or diagonal cell, with
+// the precedence of myers_backtrace_flat) until it leaves the segment's columns. Returns
+// false when the walk left the band or cost more than E (the pair is then redone).
+template <int P>
+__device__ __forceinline__ bool lane_trace_ck(const uint32_t* __restrict__ qb, const uint32_t* __restrict__ tb,
+                                              int m, int n, int nb, const LaneBand& band, const LaneGeom& g, bool act,
+                                              const uint8_t* ck, uint8_t* smem, RunWriter& rw, int* ed_out) {
+    const int lane = lane_id();
+    uint64_t* ring = reinterpret_cast<uint64_t*>(smem);
+    uint4* seg = reinterpret_cast<uint4*>(smem + kRingBytes);
+    int i = act ? m : 0, j = act ? n : 0, cost = 0;
+    bool ok = act;
+    if (g.n_max > 0) {
+        const int S = (g.n_max - 1) / kSegCols;
+        int ring_lo = lane_blo(g, S * kSegCols);  // the ring holds blocks [ring_lo, ring_lo + P]
+#pragma unroll
+        for (int k = 0; k <= P; ++k) ring_fill<P>(ring, qb, ring_lo + k, nb, lane);
+        for (int sgi = S; sgi >= 0; --sgi) {
+            const int j0 = sgi * kSegCols;
+            const int blo0 = lane_blo(g, j0);
+            if (blo0 < ring_lo) {  // one block enters the ring at the top (in the slot of ring_lo + P)
+                ring_lo = blo0;
+                ring_fill<P>(ring, qb, ring_lo, nb, lane);
+            }
+            // ---- recompute columns j0 + 1 .. min(j0 + kSegCols, n_max) ----
+            uint64_t vp[P], vn[P];
+            if (sgi == 0) {
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    vp[k] = ~0ull;
+                    vn[k] = 0;
+                }
+            } else {
+                const uint8_t* c = ck + ck_off<P>(sgi - 1, 0, lane);
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    const uint4 x = *reinterpret_cast<const uint4*>(c + k * 512);
+                    vp[k] = mk64(x.x, x.y);
+                    vn[k] = mk64(x.z, x.w);
+                }
+            }
+            int blo = blo0;
+            const int jend = min(j0 + kSegCols, g.n_max);
+            // target symbols j0 .. j0 + kSegCols - 1 share one 16-symbol word (kSegCols divides 16)
+            const int wj = j0 >> 4;
+            const uint32_t tw = wj * 16 < n ? __ldg(tb + wj) : 0u;
+            __syncwarp();  // the previous segment's walk has finished reading `seg`
+            for (int jj = j0 + 1; jj <= jend; ++jj) {  // warp-uniform
+                if (g.slide && lane_blo(g, jj) > blo) {  // the window moves down one block
+#pragma unroll
+                    for (int k = 0; k + 1 < P; ++k) {
+                        vp[k] = vp[k + 1];
+                        vn[k] = vn[k + 1];
+                    }
+                    vp[P - 1] = ~0ull;
+                    vn[P - 1] = 0;
+                    ++blo;
+                }
+                const uint32_t c = (tw >> (((jj - 1) & 15) * 2)) & 3u;
+                uint4* out = seg + (jj - j0 - 1) * (P * 32) + lane;
+                uint32_t pa = 0, ma = 0;
+#pragma unroll
+                for (int k = 0; k < P; ++k) {
+                    int rs = (blo + k) % (P + 1);
+                    const uint64_t eq = ring[(rs * 4 + c) * 32 + lane];
+                    const uint64_t ph = k == 0 ? advance_block<true>(vp[0], vn[0], eq, pa, ma)
+                                               : advance_block<false>(vp[k], vn[k], eq, pa, ma);
+                    out[k * 32] = make_uint4(lo32(vp[k]), hi32(vp[k]), lo32(ph), hi32(ph));
+                }
+            }
+            __syncwarp();
+            // ---- walk every lane through this segment's columns ----
+            for (;;) {
+                const bool want = ok && i > 0 && j > j0;
+                if (!__any_sync(PHR_FULL_MASK, want)) break;
+                if (!want) continue;
+                const int kb = ((i - 1) >> 6) - lane_blo(g, j);
+                if (kb < 0 || kb >= P) {
+                    ok = false;
+                    continue;
+                }
+                const uint4 R = seg[((j - j0 - 1) * P + kb) * 32 + lane];
+                const uint64_t vpb = mk64(R.x, R.y), hpb = mk64(R.z, R.w);
+                const int bit = (i - 1) & 63;
+                if ((vpb >> bit) & 1ull) {
+                    // D run: consecutive VP bits upward from row i within this block
+                    const int run = __clzll(~(vpb << (63 - bit)));
+                    rw.push(3, static_cast<uint32_t>(run));
+                    i -= run;
+                    cost += run;
+                } else if ((hpb >> bit) & 1ull) {
+                    rw.push(2, 1);
+                    j -= 1;
+                    cost += 1;
+                } else {
+                    const uint32_t x = sym_at<Seq2>(qb, i - 1) != sym_at<Seq2>(tb, j - 1) ? 1u : 0u;
+                    rw.push(x, 1);
+                    cost += static_cast<int>(x);
+                    i -= 1;
+                    j -= 1;
+                }
+                const int d = j - i;
+                if (d < band.dmin || d > band.dmax || cost > band.E) ok = false;
+            }
+        }
+    }
+    if (ok) {
+        if (i > 0) {
+            rw.push(3, static_cast<uint32_t>(i));
+            cost += i;
+        }
+        if (j > 0) {
+            rw.push(2, static_cast<uint32_t>(j));
+            cost += j;
+        }
+        rw.flush();
+        if (cost > band.E || rw.overflow) ok = false;
+    }
+    *ed_out = cost;
+    return ok;
+}
+
 // Forward pass and traceback of one task in one warp; records in the warp's slot. (A
 // separate traceback kernel with more resident warps measured slower on B200: the 32
 // lanes' walks diverge, so a traceback warp executes about as many instructions as the
 // forward pass whatever hides its latency.)
-template <int P>
+template <int P, bool CK>
 __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& d, bool act, const LaneBand& band,
                           const LaneGeom& g, uint64_t* sp, uint8_t* slot) {
     const int lane = lane_id();
@@ -358,19 +520,22 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     const int nb = (m + 63) >> 6;
     const uint32_t* qb = Pm.packed2 + (act ? d.q_word : 0);
     const uint32_t* tb = Pm.packed2 + (act ? d.t_word : 0);
-    lane_forward<P>(qb, tb, n, nb, g, sp, slot);
+    lane_forward<P, CK>(qb, tb, n, nb, g, sp, slot);
     // work counter: block-columns this task evaluated for its pairs
     const unsigned long long cols = __reduce_add_sync(PHR_FULL_MASK, act ? static_cast<unsigned>(n) * P : 0u);
     if (lane == 0) atomicAdd(Pm.work, cols);
     __syncwarp();  // the traceback reuses the Peq shared memory
-    const uint64_t ng = static_cast<uint64_t>((g.n_max + kLaneColGroup - 1) / kLaneColGroup);
-    const uint64_t rec_bytes = (ng * kLaneColGroup * P * 512 + 255) & ~255ull;
+    const uint64_t rec_bytes = lane_rec_bytes(g.n_max, P, CK ? 1 : 0);
     const uint32_t cap = static_cast<uint32_t>(g.m_max + g.n_max + 2);
     uint32_t* runs = reinterpret_cast<uint32_t*>(slot + rec_bytes) + static_cast<uint64_t>(lane) * cap;
     RunWriter rw;
     rw.init(runs, static_cast<uint32_t>(m + n + 2), true);
     int ed = 0;
-    const bool ok = lane_trace<P>(qb, tb, m, n, band, g, act, slot, reinterpret_cast<uint4*>(sp) + lane, rw, &ed);
+    bool ok;
+    if (CK)
+        ok = lane_trace_ck<P>(qb, tb, m, n, nb, band, g, act, slot, reinterpret_cast<uint8_t*>(sp), rw, &ed);
+    else
+        ok = lane_trace<P>(qb, tb, m, n, band, g, act, slot, reinterpret_cast<uint4*>(sp) + lane, rw, &ed);
     // work counter: pairs sent to redo
     const unsigned redo = __popc(__ballot_sync(PHR_FULL_MASK, act && !ok));
     if (lane == 0 && redo) atomicAdd(Pm.work + 1, static_cast<unsigned long long>(redo));
@@ -406,6 +571,7 @@ __device__ void lane_task(const ExtendParams& Pm, uint32_t pid, const PairDesc& 
     }
 }
 
+template <bool CK>
 __device__ __forceinline__ void lane_tasks(const ExtendParams& Pm, uint64_t* sp) {
     const int lane = lane_id();
     const uint64_t warp_global = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -430,7 +596,7 @@ __device__ __forceinline__ void lane_tasks(const ExtendParams& Pm, uint64_t* sp)
         g.nb_max = (g.m_max + 63) >> 6;
         g.P = lane_slots(g.dmin, g.dmax, g.nb_max);
         g.slide = g.P < g.nb_max;
-        const uint64_t need = lane_task_need(g.n_max, g.m_max, g.P);
+        const uint64_t need = lane_task_need(g.n_max, g.m_max, g.P, CK ? 1 : 0);
         // a task beyond the kernel's window or its warp slot is redone by the every-block kernel
         if (g.P > kLaneMaxSlots || need > Pm.slot_bytes) {
             if (lane == 0) atomicAdd(Pm.work + 1, static_cast<unsigned long long>(count));
@@ -444,29 +610,44 @@ __device__ __forceinline__ void lane_tasks(const ExtendParams& Pm, uint64_t* sp)
             continue;
         }
         switch (g.P) {
-            case 1: lane_task<1>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 2: lane_task<2>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 3: lane_task<3>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 4: lane_task<4>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 5: lane_task<5>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 6: lane_task<6>(Pm, pid, d, act, band, g, sp, slot); break;
-            case 7: lane_task<7>(Pm, pid, d, act, band, g, sp, slot); break;
-            default: lane_task<8>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 1: lane_task<1, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 2: lane_task<2, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 3: lane_task<3, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 4: lane_task<4, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 5: lane_task<5, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 6: lane_task<6, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            case 7: lane_task<7, CK>(Pm, pid, d, act, band, g, sp, slot); break;
+            default: lane_task<8, CK>(Pm, pid, d, act, band, g, sp, slot); break;
         }
         __syncwarp();
     }
 }
 
 constexpr int kLanePeqWarpBytes = kLaneMaxSlots * 4 * 32 * 8;  // Peq (and traceback buffers) per warp
+static_assert(kLanePeqWarpBytes <= kCkWarpBytes, "the forward pass's Peq must fit the checkpoint-mode area");
 
 __global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParams Pm) {
     extern __shared__ uint64_t lane_smem[];
-    lane_tasks(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kLanePeqWarpBytes / 8));
+    lane_tasks<false>(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kLanePeqWarpBytes / 8));
+}
+
+// Checkpoint mode: kCkWarpBytes of shared memory per warp, one block per SM.
+__global__ void __launch_bounds__(kLaneThreads, 1) myers_lane_ck_kernel(ExtendParams Pm) {
+    extern __shared__ uint64_t lane_smem[];
+    lane_tasks<true>(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kCkWarpBytes / 8));
 }
 
 }  // namespace
 
+int myers_lane_blocks_per_sm(int ckpt) { return ckpt ? 1 : 2; }
+
 void launch_myers_lane(const ExtendParams& p, int grid, cudaStream_t st) {
+    if (p.lane_ckpt) {
+        const int smem = kLaneWarps * kCkWarpBytes;
+        cudaFuncSetAttribute(myers_lane_ck_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        myers_lane_ck_kernel<<<grid, kLaneThreads, smem, st>>>(p);
+        return;
+    }
     const int smem = kLaneWarps * kLanePeqWarpBytes;
     cudaFuncSetAttribute(myers_lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     myers_lane_kernel<<<grid, kLaneThreads, smem, st>>>(p);

@@ -9,10 +9,13 @@
 //             :347-362, chain_cap :330-336, extend_anchor :379-404, MYERS_MAX_QUERY_LEN :248
 //   scoring   score_alignments lib.rs:170-199
 //   types     reverse_complement phraya-core/src/types.rs:91-107
-// The sketcher replaces simd-minimizers (phraya-core/src/types.rs:1848-1869), which is
-// not available to this build: canonical (DNA) / plain (protein) (k, w) minimizers with
-// the SplitMix64 finalizer as order key, leftmost minimum per window, consecutive
-// duplicates emitted once; pairs are (key, k-mer start).
+// The sketcher restates simd-minimizers 2.3.1's random minimizers
+// (phraya-core/src/types.rs:1848-1869; the crate's source is not in the reference tree)
+// from their published description: characters as packed-seq's AsciiSeq 2-bit codes
+// ((b >> 1) & 3), 32-bit ntHash order hashes (canonical: min of forward and reverse
+// complement), w-k-mer windows with the leftmost minimum, or for canonical minimizers
+// the rightmost one in windows with more A/C than T/G, each selected k-mer emitted once
+// per run of windows; pairs are (2-bit k-mer value, canonical min for DNA; position).
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 #include <cub/device/device_run_length_encode.cuh>
@@ -35,11 +38,9 @@ namespace {
 
 inline unsigned blocks_for(uint64_t n, unsigned t) { return static_cast<unsigned>((n + t - 1) / t); }
 
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
+// ntHash base seeds (Mohamadi et al. 2016), low 32 bits, indexed by the 2-bit code
+// A = 0, C = 1, T = 2, G = 3 (the complement of code c is c ^ 2).
+__constant__ uint32_t c_nt_seed[4] = {0x95c60474u, 0x62a02b4cu, 0x4be24456u, 0x82572324u};
 
 // ---------------------------------------------------------------------------
 // Sketching
@@ -67,49 +68,74 @@ __device__ __forceinline__ uint64_t find_seq(const uint64_t* base, uint64_t n, u
     return lo;
 }
 
+// Order hash of every k-mer: 32-bit ntHash over 2-bit codes, canonical = min(forward,
+// reverse complement) for DNA, forward for protein.
 __global__ void sketch_key_kernel(SketchArgs A) {
     for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_k;
          g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t s = find_seq(A.kbase, A.n, g);
         const uint64_t p = g - A.kbase[s];
         const uint8_t* b = A.seq + A.off[s] + p;
-        uint64_t v;
-        if (A.alphabet == PHR_ALPHABET_DNA) {
-            uint64_t f = 0, r = 0;
-            for (int i = 0; i < A.k; ++i) {
-                const uint64_t c = (b[i] >> 1) & 3;
-                f = (f << 2) | c;
-                r |= (c ^ 2ull) << (2 * i);
-            }
-            v = f < r ? f : r;
-        } else {
-            uint64_t f = 0;
-            for (int i = 0; i < A.k; ++i) f = (f << 8) | b[i];
-            v = f;
+        uint32_t hf = 0, hr = 0;
+        for (int i = 0; i < A.k; ++i) {
+            const uint32_t c = (b[i] >> 1) & 3u;
+            hf ^= __funnelshift_l(c_nt_seed[c], c_nt_seed[c], (A.k - 1 - i) & 31);
+            hr ^= __funnelshift_l(c_nt_seed[c ^ 2u], c_nt_seed[c ^ 2u], i & 31);
         }
-        A.key[g] = mix64(v);
+        A.key[g] = (A.alphabet == PHR_ALPHABET_DNA && hr < hf) ? hr : hf;
     }
 }
 
+// Selected k-mer of every window: the leftmost minimum hash, or for canonical (DNA)
+// minimizers the rightmost one when the window's l = w + k - 1 characters hold no more
+// T/G (codes 2, 3) than A/C.
 __global__ void sketch_window_kernel(SketchArgs A) {
+    const int l = A.w + A.k - 1;
     for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_w;
          g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t s = find_seq(A.wbase, A.n, g);
         const uint64_t p = g - A.wbase[s];
         const uint64_t* kk = A.key + A.kbase[s];
-        uint64_t best = p;
-        for (uint64_t q = p + 1; q < p + A.w; ++q)
-            if (kk[q] < kk[best]) best = q;
-        uint32_t fl = 1;
-        if (p > 0) {
-            uint64_t pb = p - 1;
-            for (uint64_t q = p; q < p - 1 + A.w; ++q)
-                if (kk[q] < kk[pb]) pb = q;
-            fl = (pb != best) ? 1u : 0u;
+        bool forward = true;
+        if (A.alphabet == PHR_ALPHABET_DNA) {
+            const uint8_t* b = A.seq + A.off[s] + p;
+            int tg = 0;
+            for (int i = 0; i < l; ++i) tg += (b[i] >> 2) & 1;  // bit 1 of the code (b >> 1) & 3
+            forward = 2 * tg > l;
         }
-        A.flag[g] = fl;
+        uint64_t best = p;
+        uint64_t bk = kk[p];
+        for (uint64_t q = p + 1; q < p + A.w; ++q) {
+            const uint64_t v = kk[q];
+            if (v < bk || (!forward && v == bk)) {
+                best = q;
+                bk = v;
+            }
+        }
         A.sel[g] = static_cast<uint32_t>(best);
     }
+}
+
+// flag = the window selects another k-mer than the window before it (first window of a
+// sequence: 1), so each selected k-mer is emitted once per run of windows.
+__global__ void sketch_flag_kernel(SketchArgs A) {
+    for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_w;
+         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t s = find_seq(A.wbase, A.n, g);
+        A.flag[g] = (g == A.wbase[s] || A.sel[g] != A.sel[g - 1]) ? 1u : 0u;
+    }
+}
+
+// 2-bit value of the k-mer at b, first character in the low bits; DNA: the smaller of
+// it and its reverse complement's.
+__device__ __forceinline__ uint64_t kmer_value(const uint8_t* b, int k, int alphabet) {
+    uint64_t vf = 0, vr = 0;
+    for (int i = 0; i < k; ++i) {
+        const uint64_t c = (b[i] >> 1) & 3u;
+        vf |= c << (2 * i);
+        vr |= (c ^ 2ull) << (2 * (k - 1 - i));
+    }
+    return (alphabet == PHR_ALPHABET_DNA && vr < vf) ? vr : vf;
 }
 
 struct SketchOut {
@@ -129,7 +155,7 @@ __global__ void sketch_scatter_kernel(SketchArgs A, const uint32_t* scan, Sketch
         const uint64_t local = scan[g] - scan[first];
         const uint64_t dst = O.remap_off ? O.remap_off[s] + local : static_cast<uint64_t>(scan[g]);
         const uint32_t b = A.sel[g];
-        O.values[dst] = A.key[A.kbase[s] + b];
+        O.values[dst] = kmer_value(A.seq + A.off[s] + b, A.k, A.alphabet);
         O.positions[dst] = b;
     }
 }
@@ -1132,6 +1158,10 @@ phr_status sketch_device(Ctx* ctx, DeviceArena& A, const uint8_t* seq, const uin
             KernelScope ks(ctx, "sketch_window");
             sketch_window_kernel<<<grid, T, 0, st>>>(S);
         }
+        {
+            KernelScope ks(ctx, "sketch_flag");
+            sketch_flag_kernel<<<grid, T, 0, st>>>(S);
+        }
         size_t ts = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, ts, S.flag, scan, static_cast<int>(TW), st);
         void* t3 = A.take(ts + 256);
@@ -2041,8 +2071,7 @@ phr_status phr_sketch_batch(phr_ctx* c, const phr_seq_batch* seqs, int32_t k, in
     phr::Ctx* ctx = &c->impl;
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
-    if (k <= 0 || w <= 0 || (alphabet == PHR_ALPHABET_DNA && k > 32) || (alphabet != PHR_ALPHABET_DNA && k > 8))
-        return phr::set_error(ctx, PHR_ERR_ARG, "k must be in 1..32 (DNA) or 1..8 (protein), w >= 1");
+    if (k <= 0 || w <= 0 || k > 32) return phr::set_error(ctx, PHR_ERR_ARG, "k must be in 1..32, w >= 1");
     const uint64_t n = seqs->n;
     if (n == 0) return PHR_OK;
     uint64_t cap_total = 0;

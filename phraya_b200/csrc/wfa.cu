@@ -661,8 +661,9 @@ __device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
 // Traceback (wfa_simd.rs:785-886) of a finished affine wavefront and the pair's result:
 // history in `auxs` through the score directory below `dir_top`. Called by all lanes of
 // the warp; the leader of each group of G lanes walks its pair.
-// With row_g > 0 the history is the register kernel's: the aux word of (score, layer, k)
-// is auxs[(score / row_g) * 3 * row_w + layer * row_w + k - row_lo], no directory read.
+// With row_g > 0 the history is the register kernel's: one word per (score, k) at
+// auxs[(score / row_g) * row_w + k - row_lo] holding raw << 4 | dop << 3 | iop << 2 | mop
+// (all three layers' history of the cell), no directory read.
 __device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int G, int qn, int tn, int X, int O,
                               int E, uint32_t* runs, const uint32_t* auxs, const AffDir* dir_top, bool done,
                               bool failed, int s_end, int t_end, int k_end, int layer_end, int row_g = 0,
@@ -670,8 +671,10 @@ __device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int
     const int gl = lane_id() & (G - 1);
     auto dir_at = [&](int64_t sc) -> const AffDir& { return dir_top[-1 - sc]; };
     auto aux_at = [&](int ss, int layer, int k) -> uint32_t {
-        if (row_g > 0)
-            return auxs[static_cast<uint64_t>(ss / row_g) * (3 * row_w) + layer * row_w + (k - row_lo)];
+        if (row_g > 0) {
+            const uint32_t w = auxs[static_cast<uint64_t>(ss / row_g) * row_w + (k - row_lo)];
+            return layer == 0 ? (((w >> 4) << 2) | (w & 3u)) : (w >> (layer + 1)) & 1u;
+        }
         const LayerBand& b = dir_at(ss).L[layer];
         return auxs[b.base + (k - b.lo)];
     };
@@ -1092,12 +1095,13 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
     const uint32_t* tb = seq_base<S>(P, d.t_word);
     const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
 
-    // region: [runs][aux rows: kRegWin words per layer per visited score]; row r holds
-    // score r * g, so the traceback needs no directory
+    // region: [runs][aux rows: kRegWin words per visited score, each word the M, I and D
+    // history of one diagonal]; row r holds score r * g, so the traceback needs no
+    // directory
     uint32_t* runs = reinterpret_cast<uint32_t*>(region);
     const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
     const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
-    const uint64_t row_cap = rest / (3 * kRegWin * 4);
+    const uint64_t row_cap = rest / (kRegWin * 4);
     uint32_t* auxs = reinterpret_cast<uint32_t*>(region + runs_bytes);
     const int wlo = max(kRegLo, -tn), whi = min(kRegLo + kRegWin - 1, qn);  // window clipped to [-tn, qn]
 
@@ -1149,7 +1153,7 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             break;
         }
         if (lane == 0) wf_cells += static_cast<uint32_t>(bhi - blo + 1);
-        uint32_t* arow = auxs + row * (3 * kRegWin);
+        uint32_t* arow = auxs + row * kRegWin;
         int32_t nM[kRegSlots], nI[kRegSlots], nD[kRegSlots];
         int best_k = INT32_MAX, best_l = 0;
 #pragma unroll
@@ -1159,6 +1163,13 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             if (klo + 31 < blo || klo > bhi) continue;  // warp-uniform: slot outside the band
             active |= 1u << h;
             const int k = klo + lane;
+            // affine_pos_valid for this diagonal as one unsigned range test: pos in
+            // [max(0, k), min(qn, tn + k)] (an empty range admits nothing; UNSET and
+            // UNSET + 1 wrap far above any span)
+            const int vl = max(0, k), vh = min(qn, tn + k);
+            const uint32_t vlo = vh >= vl ? static_cast<uint32_t>(vl) : 0x40000000u;
+            const uint32_t vspan = vh >= vl ? static_cast<uint32_t>(vh - vl) : 0u;
+            auto ok = [&](int32_t pos) { return static_cast<uint32_t>(pos) - vlo <= vspan; };
             const int32_t mo_dn = reg_neighbor<true>(M[OES - 1], h);   // M[s - O - E][k - 1]
             const int32_t ie_dn = reg_neighbor<true>(I[ES - 1], h);    // I[s - E][k - 1]
             const int32_t mo_up = reg_neighbor<false>(M[OES - 1], h);  // M[s - O - E][k + 1]
@@ -1166,42 +1177,41 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             // I (wfa_simd.rs:682-738): [open from M, extend I], strict >
             int32_t ins = UNSET;
             uint32_t iop = 0;
-            if (pos_ok(mo_dn + 1, k, qn, tn)) ins = mo_dn + 1;
-            if (pos_ok(ie_dn + 1, k, qn, tn) && ie_dn + 1 > ins) {
+            if (ok(mo_dn + 1)) ins = mo_dn + 1;
+            if (ok(ie_dn + 1) && ie_dn + 1 > ins) {
                 ins = ie_dn + 1;
                 iop = 1;
             }
             int32_t del = UNSET;
             uint32_t dop = 0;
-            if (pos_ok(mo_up, k, qn, tn)) del = mo_up;
-            if (pos_ok(de_up, k, qn, tn) && de_up > del) {
+            if (ok(mo_up)) del = mo_up;
+            if (ok(de_up) && de_up > del) {
                 del = de_up;
                 dop = 1;
             }
             // M (wfa_simd.rs:743-765): [mismatch-extend, ins close, del close], strict >
+            // (ins and del are UNSET or valid already)
             int32_t best = UNSET;
             uint32_t mop = 0;
-            if (pos_ok(M[XS - 1][h] + 1, k, qn, tn)) best = M[XS - 1][h] + 1;
-            if (pos_ok(ins, k, qn, tn) && ins > best) {
+            if (ok(M[XS - 1][h] + 1)) best = M[XS - 1][h] + 1;
+            if (ins != UNSET && ins > best) {
                 best = ins;
                 mop = 1;
             }
-            if (pos_ok(del, k, qn, tn) && del > best) {
+            if (del != UNSET && del > best) {
                 best = del;
                 mop = 2;
             }
             int32_t mval = UNSET;
-            uint32_t aux = 0;
+            uint32_t aux = (dop << 3) | (iop << 2);
             if (best != UNSET) {
                 mval = extend_valid<S>(qb, qn, tb, tn, best, k, lcp_words);
-                aux = (static_cast<uint32_t>(best) << 2) | mop;
+                aux |= (static_cast<uint32_t>(best) << 4) | mop;
             }
             nM[h] = mval;
             nI[h] = ins;
             nD[h] = del;
             arow[k - kRegLo] = aux;
-            arow[kRegWin + k - kRegLo] = iop;
-            arow[2 * kRegWin + k - kRegLo] = dop;
             // end cell: value == qn in layer order m, ins, del; smallest k (largest t_end)
             const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
             const bool cand = layer >= 0 && (fitting ? k >= qn - tn : k == qn - tn);

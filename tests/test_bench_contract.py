@@ -20,7 +20,9 @@ def bench():
 
 @pytest.fixture(scope="module")
 def sets(bench):
-    return bench.make_workload(2000, 300, seed=0)
+    from phraya_b200 import datagen as D
+    return (D.extension_pairs(2000, 100, 300, 0.05, seed=0),
+            D.extension_pairs(300, 64, 2048, 0.05, seed=1000, log_uniform=True))
 
 
 def test_roofline_fields(bench, sets):
@@ -37,8 +39,18 @@ def test_roofline_fields(bench, sets):
         # the bound is the resource with the longer lower-bound time
         assert r["bound"] == ("hbm" if r["hbm_frac"] >= r["int_frac"] else "int")
         assert r["unit"] == ("GB/s" if r["bound"] == "hbm" else "Tops/s")
+    for ckpt in (0, 1):
+        r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback", ckpt=ckpt)
+        assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
+    # traffic: from the capture record only when it was taken of the current kernel source
+    per, why = bench.traffic_record("myers_lane")
     r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")
-    assert r["traffic"] == pytest.approx(7.59e9 * set_b.n / 100000)
+    if per is None:
+        assert r["traffic"] is None and r["traffic_source"] == why
+    else:
+        assert r["traffic"] == pytest.approx(per * set_b.n)
+    assert bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback",
+                          traffic_gb=2.0)["traffic"] == pytest.approx(2.0e9)
     assert bench.roofline("pack", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")["bound"] is None
 
 

@@ -42,9 +42,13 @@ def _indel_heavy(n, seed):
     return O.PackedPairs(pairs)
 
 
+@pytest.mark.parametrize("ckpt", [1, 0])
 @pytest.mark.parametrize("band_base", [64, 16, 0])
-def test_lane_kernel_bit_exact_across_bands(band_base):
+def test_lane_kernel_bit_exact_across_bands(band_base, ckpt):
+    # ckpt 1: checkpoints every 4 columns and segments recomputed for the traceback;
+    # ckpt 0: every column's records stored
     with P.Engine(0) as eng:
+        eng.set_tune("myers_lane_ckpt", ckpt)
         eng.set_tune("myers_band_base", band_base)
         eng.set_timing(True)
         _check(eng, D.extension_pairs(2000, 64, 2048, 0.05, seed=31, log_uniform=True))
@@ -58,8 +62,10 @@ def test_lane_kernel_unrelated_pairs_redo():
     rng = np.random.default_rng(33)
     pairs = [(bytes(rng.choice(list(b"ACGT"), L).tolist()), bytes(rng.choice(list(b"ACGT"), L + d).tolist()))
              for L, d in zip(rng.integers(64, 1200, 100), rng.integers(-40, 40, 100))]
-    with P.Engine(0) as eng:
-        _check(eng, O.PackedPairs(pairs))
+    for ckpt in (1, 0):
+        with P.Engine(0) as eng:
+            eng.set_tune("myers_lane_ckpt", ckpt)
+            _check(eng, O.PackedPairs(pairs))
 
 
 def test_lane_kernel_task_tails_and_tiny_pairs():
@@ -74,5 +80,7 @@ def test_lane_kernel_task_tails_and_tiny_pairs():
             for _ in range(int(rng.integers(0, 4))):
                 t[int(rng.integers(0, len(t)))] = int(rng.choice(list(b"ACGT")))
             pairs.append((q, bytes(t)))
-        with P.Engine(0) as eng:
-            _check(eng, O.PackedPairs(pairs))
+        for ckpt in (1, 0):
+            with P.Engine(0) as eng:
+                eng.set_tune("myers_lane_ckpt", ckpt)
+                _check(eng, O.PackedPairs(pairs))

@@ -322,3 +322,38 @@ def test_anchors_from_chains_reference_cases():
     assert O.anchors(chains, A.FAST) == [100]
     assert O.anchors(chains, A.BALANCED) == [100, 5000]
     assert O.anchors(chains, A.SENSITIVE) == [100, 5000, 9000]
+
+
+def test_canonical_sketch_is_strand_symmetric():
+    """Canonical minimizers with odd l = w + k - 1 (README.md:190): a sequence and its
+    reverse complement select the same k-mers, at mirrored positions, with the same
+    canonical values (the property the window orientation rule exists for)."""
+    import random
+    rng = random.Random(5)
+    comp = bytes.maketrans(b"ACGT", b"TGCA")
+    for n in (40, 150, 1000, 5000):
+        s = bytes(rng.choice(b"ACGT") for _ in range(n))
+        v, p = O.sketch(s)
+        rv, rp = O.sketch(s.translate(comp)[::-1])
+        fwd = sorted(zip(p.tolist(), v.tolist()))
+        back = sorted((n - 21 - int(q), int(x)) for q, x in zip(rp, rv))
+        assert fwd == back, n
+        assert len(fwd) > (n - 30) * 2 // 13 if n > 100 else True
+
+
+def test_sketch_values_are_2bit_kmers():
+    """Values are the 2-bit k-mers (A=0, C=1, T=2, G=3, first character lowest); DNA
+    takes the smaller of the k-mer and its reverse complement; protein characters go
+    through the same 2-bit code."""
+    s = b"ACGTTGCAACGGTACCATGAC" * 3
+    v, p = O.sketch(s)
+    code = {ord("A"): 0, ord("C"): 1, ord("T"): 2, ord("G"): 3}
+    for val, pos in zip(v.tolist(), p.tolist()):
+        km = s[pos:pos + 21]
+        f = sum(code[c] << (2 * i) for i, c in enumerate(km))
+        r = sum((code[c] ^ 2) << (2 * (20 - i)) for i, c in enumerate(km))
+        assert val == min(f, r)
+    prot = b"MKVLAGHWEERTYIPQSDNCF" * 2
+    pv, pp = O.sketch(prot, 6, 5, A.ALPHABET_PROTEIN)
+    for val, pos in zip(pv.tolist(), pp.tolist()):
+        assert val == sum(((c >> 1) & 3) << (2 * i) for i, c in enumerate(prot[pos:pos + 6]))
