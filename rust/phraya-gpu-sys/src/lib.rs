@@ -17,7 +17,6 @@ pub const PHR_OK: i32 = 0;
 pub const PHR_INVALID_INPUT: i32 = 1;
 pub const PHR_ALIGNMENT_FAILED: i32 = 2;
 pub const PHR_ERR_OOM: i32 = 3;
-pub const PHR_ERR_TIMEOUT: i32 = 4;
 pub const PHR_ERR_CUDA: i32 = 5;
 pub const PHR_ERR_ARG: i32 = 6;
 pub const PHR_ERR_CAPACITY: i32 = 7;
