@@ -473,6 +473,9 @@ def run_engine(args, rank, world):
         t0 = time.perf_counter()
         cases["served"] = run_served(eng, dev, args, long_ref)
         cases["served"]["section_s"] = round(time.perf_counter() - t0, 1)
+        pc = cases["case2_short"]["percall_balanced_reads_per_s"]
+        if "throughput_reads_per_s" in cases["served"]["served"]:
+            cases["served"]["served_over_percall"] = cases["served"]["served"]["throughput_reads_per_s"] / pc
         eng.close()
     cpu = cpu_baseline(set_a, set_b, n_a, n_b, os.cpu_count() or 1) if not args.no_cpu else None
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
