@@ -52,11 +52,14 @@ constexpr uint8_t kBigTask = 0x80;
 constexpr int kBigThreads = 512;
 constexpr uint32_t kBigMinFrameCells = 4096;  // smallest shared frame pair worth staging
 
-// Shared-memory words the CTA-per-pair kernel needs for the two sequences of a pair
-// (one extra word each: 32-bit windows read one word past the last symbol).
+// Shared-memory words the CTA-per-pair kernel needs for the two sequences of a pair:
+// each is staged by a bulk copy from the 16-byte boundary at or below its first word
+// (up to 3 leading words) to the next 16-byte boundary, plus one zero word after it
+// (32-bit windows read one word past the last symbol), each copy starting 16-byte
+// aligned in shared memory.
 __host__ __device__ __forceinline__ uint64_t big_seq_words(int qn, int tn, int mode) {
     const int per = mode == 0 ? 16 : 4;
-    return static_cast<uint64_t>((qn + per - 1) / per + 1) + static_cast<uint64_t>((tn + per - 1) / per + 1) + 4;
+    return static_cast<uint64_t>((qn + per - 1) / per) + static_cast<uint64_t>((tn + per - 1) / per) + 16;
 }
 
 // A linear-WFA pair long enough that one warp would be latency-bound on it, whose

@@ -359,6 +359,46 @@ __device__ void wfa_linear_group(const ExtendParams& P, const PairDesc& d, uint3
 // Frames that outgrow shared memory move to the region's global frames, the same layout
 // the warp kernel uses, so scratch needs and the redo rule are identical.
 
+// Bulk asynchronous copies (the TMA unit's untiled cp.async.bulk, no multicast) of the
+// pair's sequences into shared memory, completing on an mbarrier.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// `bytes` (a positive multiple of 16) from 16-byte aligned global memory to 16-byte
+// aligned shared memory; completion is counted on `bar`.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Bounded wait for phase `parity` of `bar` (each try itself blocks for a while); false
+// when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // 32 bits holding symbols [pos, pos + kPerWord) of a sequence staged in shared memory.
 template <class S>
 __device__ __forceinline__ uint32_t window_sm(const uint32_t* base, int32_t pos) {
@@ -387,21 +427,44 @@ __device__ __forceinline__ int32_t extend_sm(const uint32_t* q, int32_t qn, cons
 
 template <class S>
 __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
-                               uint64_t region_bytes, uint32_t* sm, uint32_t sm_words, int* sh_end) {
+                               uint64_t region_bytes, uint32_t* sm, uint32_t sm_words, int* sh_end, uint64_t* bar,
+                               uint32_t& phase) {
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int qn = d.qn, tn = d.tn;
     const bool fitting = tn > qn + qn / 2 + 10;
 
     // ---- stage both sequences (plus one zero word each) in shared memory ----
+    // One bulk copy per sequence from the 16-byte boundary at or below its first word to
+    // the next 16-byte boundary after its last: the arenas are 256-byte aligned and hold
+    // four padding words after every sequence, so both ends stay inside them.
     const uint32_t* gq = seq_base<S>(P, d.q_word);
     const uint32_t* gt = seq_base<S>(P, d.t_word);
     const int qw = (qn + S::kPerWord - 1) / S::kPerWord;
     const int tw = (tn + S::kPerWord - 1) / S::kPerWord;
-    uint32_t* sq = sm;
-    uint32_t* st = sm + qw + 1;
-    for (int i = tid; i <= qw; i += nthr) sq[i] = i < qw ? __ldg(gq + i) : 0u;
-    for (int i = tid; i <= tw; i += nthr) st[i] = i < tw ? __ldg(gt + i) : 0u;
-    const uint32_t fr_off = (static_cast<uint32_t>(qw + tw + 2) + 3) & ~3u;
+    const int lead_q = static_cast<int>((reinterpret_cast<uintptr_t>(gq) & 15) >> 2);
+    const int lead_t = static_cast<int>((reinterpret_cast<uintptr_t>(gt) & 15) >> 2);
+    const uint32_t t_base = static_cast<uint32_t>(lead_q + qw + 1 + 3) & ~3u;
+    uint32_t* sq = sm + lead_q;
+    uint32_t* st = sm + t_base + lead_t;
+    const uint32_t nb_q = static_cast<uint32_t>((lead_q + qw + 3) & ~3) * 4;
+    const uint32_t nb_t = static_cast<uint32_t>((lead_t + tw + 3) & ~3) * 4;
+    if (tid == 0) {
+        // order this CTA's earlier shared-memory accesses before the async writes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, nb_q + nb_t);
+        if (nb_q) bulk_copy_g2s(sm, gq - lead_q, nb_q, bar);
+        if (nb_t) bulk_copy_g2s(sm + t_base, gt - lead_t, nb_t, bar);
+    }
+    if (!mbar_wait_bounded(bar, phase)) {
+        atomicOr(P.error_flag, 32u);
+        mbar_wait_bounded(bar, phase);  // the copies may still land: wait once more, bounded
+    }
+    phase ^= 1u;
+    if (tid == 0) {
+        sq[qw] = 0u;
+        st[tw] = 0u;
+    }
+    const uint32_t fr_off = (t_base + static_cast<uint32_t>(lead_t + tw + 1) + 3) & ~3u;
     const uint32_t fcap = sm_words > fr_off ? (sm_words - fr_off) / 2 : 0;  // cells per shared frame
     int32_t* sfr = reinterpret_cast<int32_t*>(sm + fr_off);
 
@@ -606,7 +669,11 @@ __global__ void __launch_bounds__(kBigThreads, 2) wfa_linear_big_kernel(ExtendPa
     extern __shared__ __align__(16) uint32_t big_sm[];
     __shared__ uint32_t sh_task;
     __shared__ int sh_end[3];
+    __shared__ __align__(8) uint64_t sh_bar;
     const uint32_t sm_words = P.big_smem / 4;
+    uint32_t phase = 0;  // parity of sh_bar's current phase, the same in every thread
+    if (threadIdx.x == 0) mbar_init(&sh_bar, 1);
+    __syncthreads();
     for (;;) {
         if (threadIdx.x == 0) sh_task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
         __syncthreads();
@@ -618,7 +685,7 @@ __global__ void __launch_bounds__(kBigThreads, 2) wfa_linear_big_kernel(ExtendPa
         const PairDesc d = P.desc[pid];
         if (d.mode != (S::kBits == 2 ? 0 : 1)) continue;
         wfa_linear_cta<S>(P, d, pid, P.scratch + P.task_off[task], P.task_len[task] & ~15ull, big_sm, sm_words,
-                          sh_end);
+                          sh_end, &sh_bar, phase);
     }
 }
 
