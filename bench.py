@@ -278,6 +278,29 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_one_case(args):
+    """--only-case: one read-pipeline case alone (for profiling), printed as its JSON."""
+    import torch
+
+    from phraya_b200 import api as P
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    peaks, peak_src = load_peaks()
+    int_peak = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6
+    eng = P.Engine(dev)
+    if args.only_case == "case2_short":
+        out = run_case2_short(eng, dev, args)
+    elif args.only_case == "long_reads":
+        out = run_long_reads(eng, dev, args, int_peak, peak_src)[0]
+    elif args.only_case == "contigs_protein":
+        out = run_contigs_protein(eng, dev, args)
+    else:
+        from phraya_b200 import casegen as G
+        out = run_served(eng, dev, args, G.repeat_reference(5_000_000, 20, seed=300))
+    eng.close()
+    print(json.dumps({args.only_case: out}))
+
+
 def run_engine(args, rank, world):
     import ctypes as C
 
@@ -942,6 +965,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-pipeline", action="store_true", help="skip the read-pipeline cases and serving")
     ap.add_argument("--no-contigs", action="store_true", help="skip the contig / protein case")
+    ap.add_argument("--only-case", default=None, choices=["case2_short", "long_reads", "contigs_protein", "served"],
+                    help="run one read-pipeline case alone and print its JSON (profiling); no bench line")
     ap.add_argument("--parity-pairs", type=int, default=60000,
                     help="microbench pairs of set A checked against the oracle (a tenth of that of set B)")
     ap.add_argument("--repeats", type=int, default=5, help="timed repeats of each read-pipeline call (median)")
@@ -970,7 +995,9 @@ def main():
         import torch
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if args.impl == "reference":
+        if args.only_case:
+            run_one_case(args)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_engine(args, rank, world)
