@@ -971,7 +971,7 @@ def main():
                     help="microbench pairs of set A checked against the oracle (a tenth of that of set B)")
     ap.add_argument("--repeats", type=int, default=5, help="timed repeats of each read-pipeline call (median)")
     ap.add_argument("--long-reads", type=int, default=20000, help="reads of the long-read case")
-    ap.add_argument("--long-sensitive", type=int, default=2000, help="long reads aligned under sensitive")
+    ap.add_argument("--long-sensitive", type=int, default=200, help="long reads aligned under sensitive")
     ap.add_argument("--long-parity", type=int, default=500, help="long reads checked against the oracle (balanced)")
     ap.add_argument("--long-sensitive-parity", type=int, default=16,
                     help="long reads checked against the oracle (sensitive)")
