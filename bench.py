@@ -439,6 +439,17 @@ def run_engine(args, rank, world):
     torch.cuda.synchronize()
     e2e_s = R.max_over_ranks(f0.elapsed_time(f1) / 1000.0 / args.steps, device=f"cuda:{dev}")
     h2d = 2 * input_bytes(set_a) + input_bytes(set_b)
+    # where one end-to-end step's time goes (an extra step, outside the timed region):
+    # host phases of the pipelined copies and the device kernels, per call
+    L.phr_ctx_reset_timing(eng.handle)
+    L.phr_ctx_set_timing(eng.handle, 1)
+    w0 = time.perf_counter()
+    e2e_step()
+    torch.cuda.synchronize()
+    e2e_wall_ms = (time.perf_counter() - w0) * 1e3
+    L.phr_ctx_set_timing(eng.handle, 0)
+    e2e_phases = {k: round(v[1], 2) for k, v in eng.kernel_times().items() if k.startswith("host:")}
+    e2e_kernels_ms = round(sum(v[1] for k, v in eng.kernel_times().items() if not k.startswith("host:")), 2)
 
     # parity of the timed job's own results (the last end-to-end step's host outputs) on
     # the first pairs of each set against the oracle, outside the timed regions
@@ -510,7 +521,9 @@ def run_engine(args, rank, world):
                        "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
             "gcups_dp_equivalent": gcups,
             "e2e": {"value": per_step_pairs * world / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1000.0},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1000.0,
+                    "one_step_breakdown": {"wall_ms": round(e2e_wall_ms, 2), "kernels_ms": e2e_kernels_ms,
+                                           "host_phases_ms": e2e_phases}},
             "gpu_launches": launches,
             "roofline": roof,
             "rooflines": roofs,
