@@ -30,6 +30,13 @@ METRIC = "reads/s & GCUPS on 1 B200, served vs per-call GPU; p50/p99 latency; bi
 N_A_DEFAULT = 1_000_000
 N_B_DEFAULT = 1_000_000
 COSTS_A = (4, 6, 2)
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line stays alone on stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:8.1f} s] {msg}\n")
+    sys.stderr.flush()
 
 
 def load_peaks():
@@ -349,9 +356,11 @@ def run_engine(args, rank, world):
             eng.check(L.phr_extend_batch_device(eng.handle, eng_id, C.byref(b), A.AffineCosts(*costs),
                                                 C.byref(arena)))
 
+    log(f"microbench data ready ({t_gen:.1f} s)")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    log("microbench warm-up done")
     R.barrier()
     L.phr_ctx_reset_timing(eng.handle)
     L.phr_ctx_set_timing(eng.handle, 1)
@@ -438,6 +447,7 @@ def run_engine(args, rank, world):
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_s = R.max_over_ranks(f0.elapsed_time(f1) / 1000.0 / args.steps, device=f"cuda:{dev}")
+    log(f"microbench: {ms_per_step:.2f} ms per device step, {e2e_s * 1e3:.2f} ms end to end")
     h2d = 2 * input_bytes(set_a) + input_bytes(set_b)
     # where one end-to-end step's time goes (an extra step, outside the timed region):
     # host phases of the pipelined copies and the device kernels, per call
@@ -546,13 +556,14 @@ CASE1_CMD = ("scripts/benchmark/local/gen_synthetic.py --genome-size 1000000 --n
 STRATS = ((1, "balanced"), (2, "sensitive_affine"))  # phr_strategy values
 
 
-def _median_call(fn, repeats):
+def _median_call(fn, repeats, what=""):
     """Median wall seconds of `repeats` calls (the caller has warmed up)."""
     ts = []
     for _ in range(repeats):
         t0 = time.perf_counter()
         fn()
         ts.append(time.perf_counter() - t0)
+    log(f"{what}: {repeats} calls, median {statistics.median(ts) * 1e3:.1f} ms")
     return statistics.median(ts), ts
 
 
@@ -623,7 +634,7 @@ def run_case2_short(eng, dev, args):
     for strat, name in STRATS:
         call = lambda: eng.align_packed(idx, packed, strat, A.GAP_AFFINE)  # noqa: E731
         res = call()  # warm-up, and the results checked below
-        med, ts = _median_call(call, args.repeats)
+        med, ts = _median_call(call, args.repeats, f"case2 {name}")
         kms, _ = _kernel_split(eng, call)
         gpu[name] = P.unpack_reads(*res[:3])
         out[name] = {"reads_per_s": packed.n / med, "aligned_bases_per_s": _aligned_bases(packed, res[0]) / med,
@@ -657,6 +668,7 @@ def run_case2_short(eng, dev, args):
         cores = os.cpu_count() or 1
         for strat, name in STRATS:
             rows, ost, secs = _oracle_batches(otg, packed, strat, cores)
+            log(f"case2 {name}: oracle {secs:.1f} s")
             out[name]["parity"] = _read_parity(gpu[name], rows)
             out[name]["parity"]["stats_equal"] = tuple(ost) == tuple(out[name]["stats"])
             out[name]["cpu_baseline"] = {"value": packed.n / secs, "unit": "reads/s", "cores": cores, "kind": "port",
@@ -702,6 +714,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
     ref = G.repeat_reference(5_000_000, 20, seed=300)
     packed, _, _ = G.long_reads(ref, args.long_reads, seed=301)
     gen_s = time.perf_counter() - t0
+    log(f"long reads generated in {gen_s:.1f} s")
     idx = eng.index(ref)
     out = {"workload": "long-read Case 2: 5 Mbp genome + 20 repeat copies (1-5 kb, 0.5 % divergence); reads "
                        "lognormal (median 8 kb, sigma 0.5, 1-50 kb), 5 % error (60 % indels, 40 % substitutions)",
@@ -711,7 +724,8 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
     clocks.start()
     call = lambda: eng.align_packed(idx, packed, A.BALANCED, A.GAP_AFFINE)  # noqa: E731
     res = call()
-    med, ts = _median_call(call, max(1, args.repeats // 2))
+    log("long balanced: first call done")
+    med, ts = _median_call(call, max(1, args.repeats // 2), "long balanced")
     kms, work = _kernel_split(eng, call)
     out["balanced"] = {"reads_per_s": packed.n / med, "aligned_bases_per_s": _aligned_bases(packed, res[0]) / med,
                        "ms_per_call_median": med * 1e3, "ms_per_call": [round(t * 1e3, 1) for t in ts],
@@ -727,6 +741,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
     t1 = time.perf_counter()
     scall()
     sdt = time.perf_counter() - t1
+    log(f"long sensitive ({ns} reads): {sdt * 1e3:.1f} ms per call")
     skms, swork = _kernel_split(eng, scall)
     out["sensitive_affine"] = {"reads": ns, "reads_per_s": ns / sdt, "aligned_bases_per_s":
                                _aligned_bases(sub, sres[0]) / sdt, "ms_per_call": sdt * 1e3, "stats": list(sres[3]),
@@ -741,6 +756,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
         cores = os.cpu_count() or 1
         pick = list(range(0, packed.n, max(1, packed.n // args.long_parity)))[:args.long_parity]
         rows, _, secs = _oracle_batches(otg, packed.subset(pick), A.BALANCED, cores)
+        log(f"long balanced: oracle {secs:.1f} s")
         out["balanced"]["parity"] = _read_parity(gpu_bal, rows, pick)
         out["balanced"]["cpu_baseline"] = {"value": len(pick) / secs, "unit": "reads/s", "cores": cores,
                                            "kind": "port", "sample": f"{len(pick)} of {packed.n} reads (every "
@@ -748,6 +764,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
                                                                      f"{secs:.1f} s"}
         spick = list(range(min(args.long_sensitive_parity, ns)))
         rows, _, secs = _oracle_batches(otg, sub.subset(spick), A.SENSITIVE, cores)
+        log(f"long sensitive: oracle {secs:.1f} s")
         out["sensitive_affine"]["parity"] = _read_parity(gpu_sens, rows, spick)
         out["sensitive_affine"]["cpu_baseline"] = {"value": len(spick) / secs, "unit": "reads/s", "cores": cores,
                                                    "kind": "port", "sample": f"first {len(spick)} reads, {secs:.1f} s"}
@@ -794,7 +811,8 @@ def run_contigs_protein(eng, dev, args):
     clocks.start()
     call = lambda: eng.align_packed(idx, packed, A.BALANCED, A.GAP_AFFINE)  # noqa: E731
     res = call()
-    med, ts = _median_call(call, max(1, args.repeats // 2))
+    log("contigs: first call done")
+    med, ts = _median_call(call, max(1, args.repeats // 2), "contigs")
     kms, _ = _kernel_split(eng, call)
     out["contigs"].update({"contigs_per_s": len(contigs) / med, "aligned_bases_per_s": _aligned_bases(packed, res[0]) / med,
                            "ms_per_call_median": med * 1e3, "ms_per_call": [round(t * 1e3, 1) for t in ts],
@@ -811,7 +829,7 @@ def run_contigs_protein(eng, dev, args):
     for name, e in engines:
         pcall = lambda: eng.extend_packed(e, pp, P.AffineCosts(2, 4, 1))  # noqa: E731
         r = pcall()
-        pm, _ = _median_call(pcall, args.repeats)
+        pm, _ = _median_call(pcall, args.repeats, f"protein {name}")
         gpu_p[name] = r
         prot[name] = {"pairs_per_s": pp.n / pm, "ms_per_call_median": pm * 1e3}
     # align_read in protein space: the first 1,000 queries against their 1,000 targets
@@ -823,7 +841,7 @@ def run_contigs_protein(eng, dev, args):
     pidx = eng.index(proteome, alphabet=A.ALPHABET_PROTEIN)
     acall = lambda: eng.align_packed(pidx, queries, A.BALANCED, A.GAP_AFFINE)  # noqa: E731
     pres = acall()
-    am, _ = _median_call(acall, max(1, args.repeats // 2))
+    am, _ = _median_call(acall, max(1, args.repeats // 2), "protein align_read")
     prot["align_read"] = {"workload": f"{n_pa} queries against their {n_pa} targets concatenated "
                                       f"({len(proteome)} aa; k6/w5, no reverse strand), balanced",
                           "reads_per_s": queries.n / am, "ms_per_call_median": am * 1e3, "stats": list(pres[3])}
@@ -868,6 +886,7 @@ def run_contigs_protein(eng, dev, args):
             pool.terminate()
             pool.join()
         pick = sorted(done)
+        log(f"contigs: oracle finished {len(pick)} of {len(contigs)}")
         par = _read_parity(gpu_c, [done[i][0] for i in pick], pick)
         par["contigs_not_finished_by_oracle"] = len(contigs) - len(pick)
         par["oracle_deadline_s"] = args.contig_oracle_s
@@ -905,7 +924,7 @@ def run_served(eng, dev, args, ref):
     packed = PackedReads(stream)
     call = lambda: eng.align_packed(idx, packed, A.BALANCED, A.GAP_AFFINE)  # noqa: E731
     bres = call()
-    med, _ = _median_call(call, max(1, args.repeats // 2))
+    med, _ = _median_call(call, max(1, args.repeats // 2), "served stream batched")
     batched = P.unpack_reads(*bres[:3])
     out = {"workload": "served mixed stream on the 5 Mbp long-read genome: Poisson arrivals, 90 % 150 bp reads "
                        "(1 % error), 10 % lognormal long reads (median 8 kb, 5 % error), balanced",
@@ -941,6 +960,7 @@ def run_served(eng, dev, args, ref):
         sl = sorted(lat[j] for j in range(n) if is_short[j])
         al = sorted(lat.values())
         mism = sum(1 for j in range(n) if res[j] != batched[j])
+        log(f"served {rate:.0f}/s repeat {rep}: {n} reads in {t_total:.2f} s")
         return {"rate_offered_reads_per_s": rate, "repeat": rep, "reads": n,
                 "long_reads": int((~is_short[:n]).sum()), "throughput_reads_per_s": n / t_total,
                 "p50_ms_150bp": sl[len(sl) // 2] / 1000.0, "p99_ms_150bp": sl[min(len(sl) - 1, int(len(sl) * 0.99))] / 1000.0,
