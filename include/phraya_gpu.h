@@ -190,7 +190,12 @@ void* phr_ctx_stream(const phr_ctx* ctx);
  * Aligns every pair of `batch` (host memory) with `engine` and writes one
  * phr_alignment per pair plus packed CIGAR text into `out` (host memory).
  * `costs` is read only by PHR_ENGINE_WFA_AFFINE. Pairs are independent; per-pair
- * failures are reported in phr_alignment.status, the call itself returns PHR_OK.
+ * failures are reported in phr_alignment.status, the call itself returns PHR_OK. A pair
+ * whose extension needs more scratch than the context's workspace budget (a very
+ * divergent pair of very long sequences: the reference's own full-width history would
+ * need more memory still) reports PHR_ERR_OOM in its status and no alignment; align_read
+ * skips such an anchor as it skips a failed extension (executor.rs:558). The context
+ * counter "scratch_oom_pairs" counts them.
  */
 phr_status phr_extend_batch(phr_ctx* ctx, phr_engine engine, const phr_pair_batch* batch,
                             phr_affine_costs costs, phr_result_arena* out);
@@ -557,7 +562,8 @@ typedef struct {
     uint32_t max_wait_us;          /* batch-forming window after first arrival     */
     uint32_t n_streams;            /* concurrent batches in flight (0 = 2)         */
     int32_t short_lane;            /* worker 0 takes only reads <= 500 bases, on a
-                                      high-priority stream: 0 = on when n_streams >= 2,
+                                      high-priority stream, and the other workers
+                                      only longer reads: 0 = on when n_streams >= 2,
                                       1 = on, -1 = off                               */
     uint32_t long_blocks_per_sm;   /* resident blocks per SM of the extension kernels
                                       of the other workers while a short lane runs

@@ -573,7 +573,7 @@ __global__ void finish_kernel(FinishParams F) {
                 a.query_end = static_cast<uint32_t>(d.qn);
                 a.target_start = 0;
                 a.target_end = static_cast<uint32_t>(d.tn);
-            } else if (o.status == PHR_INVALID_INPUT || o.status == PHR_ALIGNMENT_FAILED) {
+            } else if (o.status != PHR_OK) {
                 a.query_start = a.query_end = a.target_start = a.target_end = 0;
             } else {
                 a.query_start = static_cast<uint32_t>(d.qs);
@@ -927,6 +927,10 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     std::vector<uint32_t> h_list;
     std::vector<unsigned long long> h_rneed;
     std::unordered_set<uint32_t> clamped;
+    // a pair that still overflows the whole budget ends with status PHR_ERR_OOM (the
+    // other pairs of the call go on)
+    static const PairOut kOomOut = {PHR_ERR_OOM, 0, 0, 0, 0, 0};
+    uint64_t n_oom = 0;
     HostScope hs_redo(ctx, "host:redo");
     for (int round = 0; round < 12; ++round) {
         uint32_t h_redo = 0;
@@ -953,8 +957,13 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                 uint64_t need = (std::max<uint64_t>(h_rneed[idx[pos]], 4096) + 255) & ~255ull;
                 if (need > ctx->scratch_budget) {
                     // first-pass needs are estimates: try once with the whole budget
-                    if (clamped.count(h_list[idx[pos]]))
-                        return set_error(ctx, PHR_ERR_OOM, "a single pair needs more scratch than the workspace budget");
+                    if (clamped.count(h_list[idx[pos]])) {
+                        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(pout + h_list[idx[pos]], &kOomOut, sizeof(PairOut),
+                                                          cudaMemcpyHostToDevice, st));
+                        ++n_oom;
+                        ++pos;
+                        continue;
+                    }
                     clamped.insert(h_list[idx[pos]]);
                     need = ctx->scratch_budget & ~255ull;
                 }
@@ -966,6 +975,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                 ++pos;
             }
             const uint32_t m = static_cast<uint32_t>(pl.size());
+            if (m == 0) continue;
             PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rlist2, pl.data(), m * 4, cudaMemcpyHostToDevice, st));
             PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rtask_off, po.data(), m * 8, cudaMemcpyHostToDevice, st));
             PHR_CUDA_TRY(ctx, cudaMemcpyAsync(rtask_len, pn.data(), m * 8, cudaMemcpyHostToDevice, st));
@@ -994,6 +1004,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
     }
 
     hs_redo.stop();
+    if (n_oom) ctx->counters["scratch_oom_pairs"] += n_oom;
     HostScope hs_tail(ctx, "host:extend_tail");
     // pack CIGAR text
     {

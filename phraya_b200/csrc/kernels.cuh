@@ -128,11 +128,18 @@ constexpr int kSegCols = 4;
 // Scratch of one lane task, then one reverse-run list of (m_max + n_max + 2) words per
 // lane. Record mode: 16-byte {VP, HP} records [column group][slot][lane][column in
 // group] of every column. Checkpoint mode: 16-byte {VP, VN} states [checkpoint][slot]
-// [lane] after columns kSegCols, 2 kSegCols, ... below n_max.
+// [lane] after columns kSegCols, 2 kSegCols, ... below n_max, then the traceback's
+// segment buffer: the {VP, HP} records of one segment [column][slot][lane] (rewritten
+// every segment, so it stays in the caches).
+__host__ __device__ __forceinline__ uint64_t lane_ckpt_bytes(int n_max, int P) {
+    const uint64_t nck = n_max > 0 ? static_cast<uint64_t>((n_max - 1) / kSegCols) : 0;
+    return (nck * P * 512 + 255) & ~255ull;
+}
+
 __host__ __device__ __forceinline__ uint64_t lane_rec_bytes(int n_max, int P, int ckpt) {
     const uint64_t ng = static_cast<uint64_t>((n_max + kLaneColGroup - 1) / kLaneColGroup);
-    const uint64_t nck = n_max > 0 ? static_cast<uint64_t>((n_max - 1) / kSegCols) : 0;
-    return ckpt ? ((nck * P * 512 + 255) & ~255ull) : ((ng * kLaneColGroup * P * 512 + 255) & ~255ull);
+    return ckpt ? lane_ckpt_bytes(n_max, P) + static_cast<uint64_t>(kSegCols) * P * 512
+                : ((ng * kLaneColGroup * P * 512 + 255) & ~255ull);
 }
 
 __host__ __device__ __forceinline__ uint64_t lane_task_need(int n_max, int m_max, int P, int ckpt = 0) {

@@ -363,10 +363,12 @@ __device__ __forceinline__ bool lane_trace(const uint32_t* __restrict__ qb, cons
 }
 
 // Shared memory of one warp in checkpoint mode: the Peq ring (kLaneMaxSlots + 1 blocks,
-// [block % (P + 1)][base][lane], 64-bit masks) then one segment's {VP, HP} records
-// [column][slot][lane]. The forward pass's Peq ([slot][base][lane]) reuses its start.
+// [block % (P + 1)][base][lane], 64-bit masks). The forward pass's Peq ([slot][base]
+// [lane]) reuses its start. The segment's records live in the warp's scratch slot: each
+// lane writes and reads back only its own, a few KB per warp that stay in L1/L2, and
+// shared memory stays small enough for two blocks per SM.
 constexpr int kRingBytes = (kLaneMaxSlots + 1) * 4 * 32 * 8;
-constexpr int kCkWarpBytes = kRingBytes + kSegCols * kLaneMaxSlots * 32 * 16;
+constexpr int kCkWarpBytes = kRingBytes;
 
 // Peq of query block b (zero past the query) into ring slot b % (P + 1).
 template <int P>
@@ -392,10 +394,10 @@ __device__ __forceinline__ void ring_fill(uint64_t* ring, const uint32_t* __rest
 template <int P>
 __device__ __forceinline__ bool lane_trace_ck(const uint32_t* __restrict__ qb, const uint32_t* __restrict__ tb,
                                               int m, int n, int nb, const LaneBand& band, const LaneGeom& g, bool act,
-                                              const uint8_t* ck, uint8_t* smem, RunWriter& rw, int* ed_out) {
+                                              uint8_t* ck, uint8_t* smem, RunWriter& rw, int* ed_out) {
     const int lane = lane_id();
     uint64_t* ring = reinterpret_cast<uint64_t*>(smem);
-    uint4* seg = reinterpret_cast<uint4*>(smem + kRingBytes);
+    uint4* seg = reinterpret_cast<uint4*>(ck + lane_ckpt_bytes(g.n_max, P));
     int i = act ? m : 0, j = act ? n : 0, cost = 0;
     bool ok = act;
     if (g.n_max > 0) {
@@ -432,7 +434,7 @@ __device__ __forceinline__ bool lane_trace_ck(const uint32_t* __restrict__ qb, c
             // target symbols j0 .. j0 + kSegCols - 1 share one 16-symbol word (kSegCols divides 16)
             const int wj = j0 >> 4;
             const uint32_t tw = wj * 16 < n ? __ldg(tb + wj) : 0u;
-            __syncwarp();  // the previous segment's walk has finished reading `seg`
+            // (each lane reads back only the records it wrote: no barrier is needed)
             for (int jj = j0 + 1; jj <= jend; ++jj) {  // warp-uniform
                 if (g.slide && lane_blo(g, jj) > blo) {  // the window moves down one block
 #pragma unroll
@@ -631,15 +633,15 @@ __global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_kernel(ExtendParam
     lane_tasks<false>(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kLanePeqWarpBytes / 8));
 }
 
-// Checkpoint mode: kCkWarpBytes of shared memory per warp, one block per SM.
-__global__ void __launch_bounds__(kLaneThreads, 1) myers_lane_ck_kernel(ExtendParams Pm) {
+// Checkpoint mode: kCkWarpBytes of shared memory per warp, two blocks per SM.
+__global__ void __launch_bounds__(kLaneThreads, 2) myers_lane_ck_kernel(ExtendParams Pm) {
     extern __shared__ uint64_t lane_smem[];
     lane_tasks<true>(Pm, lane_smem + static_cast<uint64_t>(threadIdx.x >> 5) * (kCkWarpBytes / 8));
 }
 
 }  // namespace
 
-int myers_lane_blocks_per_sm(int ckpt) { return ckpt ? 1 : 2; }
+int myers_lane_blocks_per_sm(int) { return 2; }
 
 void launch_myers_lane(const ExtendParams& p, int grid, cudaStream_t st) {
     if (p.lane_ckpt) {

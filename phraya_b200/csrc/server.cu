@@ -299,10 +299,12 @@ void run_scheduler(phr_server* S) {
     auto pick = [&](const phr_server::Worker* w) -> int {
         const bool s0 = !S->pending[0].empty(), s1 = !S->pending[1].empty();
         if (w->short_only) return s0 ? 0 : -1;
+        // with a short lane, short reads are its alone: on a general worker a short batch
+        // shares the SMs with long-read kernels on a low-priority stream and can wait for
+        // them for tens of milliseconds
+        if (S->short_lane) return s1 ? 1 : -1;
         if (s0 && s1) return S->pending[1].front().t0 < S->pending[0].front().t0 ? 1 : 0;
         if (s1) return 1;
-        // short reads go to a general worker only while the short lane is busy
-        if (s0 && S->short_lane && !S->workers[0]->busy) return -1;
         return s0 ? 0 : -1;
     };
     auto ready = [&]() -> bool {

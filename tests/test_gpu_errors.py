@@ -1,5 +1,5 @@
 """Failure paths of the C ABI that are made on the host: a scratch budget too small for
-one pair ends the call with PHR_ERR_OOM and a message, and the context stays usable;
+one pair gives that pair PHR_ERR_OOM while the rest of the call is aligned;
 bad arguments are refused with PHR_ERR_ARG before any work; a result arena too small
 for the CIGAR text gives PHR_ERR_CAPACITY. No kernel is made to fail."""
 import ctypes as C
@@ -23,13 +23,18 @@ def divergent_pair(n, seed):
     return q, t
 
 
-def test_workspace_too_small_is_oom_and_context_survives():
+def test_workspace_too_small_is_per_pair_oom():
+    """A pair whose extension needs more scratch than the budget reports PHR_ERR_OOM in
+    its own status; the other pairs of the call are aligned, and the context goes on."""
     small = D.extension_pairs(64, 100, 300, 0.05, seed=31)
-    with P.Engine(0, workspace_bytes=1 << 16) as eng:
-        with pytest.raises(P.EngineError) as ei:
-            eng.extend(A.ENGINE_WFA_LINEAR, [divergent_pair(20000, 1)])
-        assert ei.value.status == A.PHR_ERR_OOM
-        assert "scratch" in str(ei.value)
+    pairs = [(bytes(small.seq[int(small.q_off[i]):int(small.q_off[i]) + int(small.q_len[i])]),
+              bytes(small.seq[int(small.t_off[i]):int(small.t_off[i]) + int(small.t_len[i])])) for i in range(8)]
+    with P.Engine(0, workspace_bytes=1 << 20) as eng:
+        got = eng.extend(A.ENGINE_WFA_LINEAR, pairs[:4] + [divergent_pair(20000, 1)] + pairs[4:])
+        assert got[4][0] == A.PHR_ERR_OOM and got[4][1] == ""
+        want = O.extend(A.ENGINE_WFA_LINEAR, pairs)
+        assert got[:4] + got[5:] == want
+        assert eng.counter("scratch_oom_pairs") == 1
         # the same context still aligns pairs that fit its budget
         ga, gc = eng.extend_packed(A.ENGINE_WFA_AFFINE, small, P.AffineCosts(4, 6, 2))
         oa, oc = O.extend_packed(A.ENGINE_WFA_AFFINE, small, (4, 6, 2))
