@@ -899,7 +899,8 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             else
                 launch_wfa_affine_bytes(P, static_cast<int>(grid), block, st);
         }
-        if (per_task && engine == PHR_ENGINE_WFA_LINEAR && P.big_min > 0 && n_tasks_hint > 0) {
+        if (per_task && (engine == PHR_ENGINE_WFA_LINEAR || engine == PHR_ENGINE_WFA_AFFINE) && P.big_min > 0 &&
+            n_tasks_hint > 0) {
             // long pairs of this redo list, one CTA each
             const uint64_t big_per_sm = ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1;
             const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, ctx->sm_count * big_per_sm));
@@ -907,8 +908,13 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             for (int mode = 0; mode < 2; ++mode) {
                 P.tasks.range = mode ? range1 : range0;
                 P.queue_head = cnt + 24 + mode;
-                KernelScope ks(ctx, mode ? "wfa_linear_big_bytes" : "wfa_linear_big");
-                launch_wfa_linear_big(P, big_grid, mode, st);
+                if (engine == PHR_ENGINE_WFA_LINEAR) {
+                    KernelScope ks(ctx, mode ? "wfa_linear_big_bytes" : "wfa_linear_big");
+                    launch_wfa_linear_big(P, big_grid, mode, st);
+                } else {
+                    KernelScope ks(ctx, mode ? "wfa_affine_big_bytes" : "wfa_affine_big");
+                    launch_wfa_affine_big(P, big_grid, mode, st);
+                }
             }
         }
         PHR_CUDA_TRY(ctx, cudaGetLastError());

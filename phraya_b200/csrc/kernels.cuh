@@ -62,11 +62,12 @@ __host__ __device__ __forceinline__ uint64_t big_seq_words(int qn, int tn, int m
     return static_cast<uint64_t>((qn + per - 1) / per) + static_cast<uint64_t>((tn + per - 1) / per) + 16;
 }
 
-// A linear-WFA pair long enough that one warp would be latency-bound on it, whose
-// sequences fit the CTA's shared memory with room for frames.
+// A WFA pair (linear or gap-affine) long enough that one warp would be latency-bound on
+// it, whose sequences fit the CTA's shared memory with room for (linear) frames.
 __host__ __device__ __forceinline__ bool big_pair(int32_t engine, int32_t big_min, uint32_t big_smem, int qn, int tn,
                                                   int mode) {
-    if (big_min <= 0 || engine != PHR_ENGINE_WFA_LINEAR || qn + tn < big_min) return false;
+    if (big_min <= 0 || (engine != PHR_ENGINE_WFA_LINEAR && engine != PHR_ENGINE_WFA_AFFINE) || qn + tn < big_min)
+        return false;
     return (big_seq_words(qn, tn, mode) + 2ull * kBigMinFrameCells) * 4 <= big_smem;
 }
 
@@ -165,5 +166,6 @@ constexpr int kLaneThreads = 256;
 void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
+void launch_wfa_affine_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
 
 }  // namespace phr

@@ -425,22 +425,20 @@ __device__ __forceinline__ int32_t extend_sm(const uint32_t* q, int32_t qn, cons
     return q_pos + lim;
 }
 
+// Stages a pair's two sequences in the CTA's shared memory `sm`, each followed by one
+// zero word (32-bit windows read one word past the last symbol): one bulk copy per
+// sequence from the 16-byte boundary at or below its first word to the next 16-byte
+// boundary after its last (the arenas are 256-byte aligned and hold four padding words
+// after every sequence, so both ends stay inside them). Called by every thread of the
+// CTA; returns the first free word after the staged sequences (16-byte aligned).
 template <class S>
-__device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
-                               uint64_t region_bytes, uint32_t* sm, uint32_t sm_words, int* sh_end, uint64_t* bar,
-                               uint32_t& phase) {
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int qn = d.qn, tn = d.tn;
-    const bool fitting = tn > qn + qn / 2 + 10;
-
-    // ---- stage both sequences (plus one zero word each) in shared memory ----
-    // One bulk copy per sequence from the 16-byte boundary at or below its first word to
-    // the next 16-byte boundary after its last: the arenas are 256-byte aligned and hold
-    // four padding words after every sequence, so both ends stay inside them.
+__device__ uint32_t stage_pair_cta(const ExtendParams& P, const PairDesc& d, uint32_t* sm, uint64_t* bar,
+                                   uint32_t& phase, uint32_t** sq_out, uint32_t** st_out) {
+    const int tid = threadIdx.x;
     const uint32_t* gq = seq_base<S>(P, d.q_word);
     const uint32_t* gt = seq_base<S>(P, d.t_word);
-    const int qw = (qn + S::kPerWord - 1) / S::kPerWord;
-    const int tw = (tn + S::kPerWord - 1) / S::kPerWord;
+    const int qw = (d.qn + S::kPerWord - 1) / S::kPerWord;
+    const int tw = (d.tn + S::kPerWord - 1) / S::kPerWord;
     const int lead_q = static_cast<int>((reinterpret_cast<uintptr_t>(gq) & 15) >> 2);
     const int lead_t = static_cast<int>((reinterpret_cast<uintptr_t>(gt) & 15) >> 2);
     const uint32_t t_base = static_cast<uint32_t>(lead_q + qw + 1 + 3) & ~3u;
@@ -464,7 +462,24 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
         sq[qw] = 0u;
         st[tw] = 0u;
     }
-    const uint32_t fr_off = (t_base + static_cast<uint32_t>(lead_t + tw + 1) + 3) & ~3u;
+    *sq_out = sq;
+    *st_out = st;
+    return (t_base + static_cast<uint32_t>(lead_t + tw + 1) + 3) & ~3u;
+}
+
+template <class S>
+__device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
+                               uint64_t region_bytes, uint32_t* sm, uint32_t sm_words, int* sh_end, uint64_t* bar,
+                               uint32_t& phase) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int qn = d.qn, tn = d.tn;
+    const bool fitting = tn > qn + qn / 2 + 10;
+
+    // ---- stage both sequences (plus one zero word each) in shared memory ----
+    uint32_t *sq, *st;
+    const uint32_t fr_off = stage_pair_cta<S>(P, d, sm, bar, phase, &sq, &st);
+    const int qw = (qn + S::kPerWord - 1) / S::kPerWord;
+    const int tw = (tn + S::kPerWord - 1) / S::kPerWord;
     const uint32_t fcap = sm_words > fr_off ? (sm_words - fr_off) / 2 : 0;  // cells per shared frame
     int32_t* sfr = reinterpret_cast<int32_t*>(sm + fr_off);
 
@@ -1111,6 +1126,258 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
 }
 
 // ===========================================================================
+// Gap-affine WFA, one CTA per long pair
+// ===========================================================================
+// The warp-group kernel above runs a long, divergent pair with 32 lanes over bands of
+// thousands of diagonals per score, and only a few hundred such pairs exist in a batch:
+// most SMs idle. Here a CTA of kBigThreads threads takes one pair; the recurrence, cell
+// layout, band directory, candidate order and tie-breaks are those of wfa_affine_group
+// (values, ops and the end cell are identical), the diagonals of each score are dealt to
+// the CTA's threads, both sequences sit in shared memory (bulk copies), and one warp
+// walks the traceback.
+template <class S>
+__device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
+                               uint64_t region_bytes, uint32_t* sm, uint64_t* bar, uint32_t& phase, int* sh_red) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int qn = d.qn, tn = d.tn;
+    const bool fitting = tn > qn + qn / 2 + 10;
+    const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
+    const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
+    uint32_t *qb, *tb;
+    stage_pair_cta<S>(P, d, sm, bar, phase, &qb, &tb);
+
+    // region layout of wfa_affine_group: [runs][values][aux][... directory growing down]
+    uint32_t* runs = reinterpret_cast<uint32_t*>(region);
+    const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
+    const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
+    const uint64_t dir_cap = (rest / 4) / sizeof(AffDir);
+    const uint64_t cell_bytes = rest - rest % sizeof(AffDir) - dir_cap * sizeof(AffDir);
+    const uint64_t cell_cap = min(static_cast<uint64_t>((cell_bytes / 8) & ~3ull), static_cast<uint64_t>(0xFFFFFFFFu));
+    int32_t* vals = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* auxs = reinterpret_cast<uint32_t*>(vals + cell_cap);
+    AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + rest - (rest % sizeof(AffDir)));
+    auto dir_at = [&](int64_t sc) -> AffDir& { return dir_top[-1 - sc]; };
+    auto fits = [&](uint64_t ncells, int64_t nscores) -> bool {
+        return ncells <= cell_cap && static_cast<uint64_t>(nscores) <= dir_cap;
+    };
+    auto band_of = [&](int64_t sc, int layer) -> SBand {
+        const LayerBand& b = dir_at(sc).L[layer];
+        return SBand{b.lo, b.hi, static_cast<uint32_t>(b.base)};
+    };
+
+    bool done = false, overflow = false;
+    int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
+    uint32_t used = 0;
+    uint32_t wf_cells = 0, lcp_words = 0;
+    if (dir_cap < 1 || cell_cap < 1 || !fits(1, 1)) overflow = true;
+    // ---- s = 0 ----
+    if (!overflow && tid == 0) {
+        AffDir e;
+        e.L[0] = LayerBand{0, 0, 0};
+        e.L[1] = LayerBand{1, 0, 1};
+        e.L[2] = LayerBand{1, 0, 1};
+        dir_at(0) = e;
+        vals[0] = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
+        auxs[0] = 0;
+    }
+    __syncthreads();
+    if (!overflow) {
+        used = 1;
+        const int v0 = vals[0];
+        if (!fitting) {
+            if (qn - tn == 0 && v0 == qn) {
+                done = true;
+                t_end = tn;
+            }
+        } else if (qn <= tn && v0 == qn) {
+            done = true;
+            t_end = qn;
+        }
+    }
+    const SBand none = {1, 0, 0u};
+    int g = 0;
+    for (int v : {X, O, E}) {
+        int a = g, b = v < 0 ? -v : v;
+        while (b) {
+            const int t = a % b;
+            a = b;
+            b = t;
+        }
+        g = a;
+    }
+    const int step = g > 0 ? g : 1;
+    int64_t s = step;
+    // every thread computes the same bands and counters from the directory, so control
+    // flow is uniform across the CTA
+    while (!done && !overflow && s <= hard_max_s) {
+        SBand bI = none, bD = none, bM = none;
+        SBand sMo = none, sIe = none, sDe = none, sMx = none;
+        const int64_t so = s - O - E, se = s - E, sx = s - X;
+        if (so >= 0) sMo = band_of(so, 0);
+        if (se >= 0) {
+            sIe = band_of(se, 1);
+            sDe = band_of(se, 2);
+        }
+        if (sx >= 0) sMx = band_of(sx, 0);
+        int lo = INT32_MAX, hi = INT32_MIN;
+        if (sMo.lo <= sMo.hi) { lo = min(lo, sMo.lo + 1); hi = max(hi, sMo.hi + 1); }
+        if (sIe.lo <= sIe.hi) { lo = min(lo, sIe.lo + 1); hi = max(hi, sIe.hi + 1); }
+        bI.lo = max(lo, -tn);
+        bI.hi = min(hi, qn);
+        lo = INT32_MAX;
+        hi = INT32_MIN;
+        if (sMo.lo <= sMo.hi) { lo = min(lo, sMo.lo - 1); hi = max(hi, sMo.hi - 1); }
+        if (sDe.lo <= sDe.hi) { lo = min(lo, sDe.lo - 1); hi = max(hi, sDe.hi - 1); }
+        bD.lo = max(lo, -tn);
+        bD.hi = min(hi, qn);
+        lo = INT32_MAX;
+        hi = INT32_MIN;
+        if (sMx.lo <= sMx.hi) { lo = min(lo, sMx.lo); hi = max(hi, sMx.hi); }
+        if (bI.lo <= bI.hi) { lo = min(lo, bI.lo); hi = max(hi, bI.hi); }
+        if (bD.lo <= bD.hi) { lo = min(lo, bD.lo); hi = max(hi, bD.hi); }
+        bM.lo = max(lo, -tn);
+        bM.hi = min(hi, qn);
+        if (tid == 0 && bM.lo <= bM.hi) wf_cells += static_cast<uint32_t>(bM.hi - bM.lo + 1);
+        const uint32_t wI = bI.lo <= bI.hi ? static_cast<uint32_t>(bI.hi - bI.lo + 1) : 0;
+        const uint32_t wD = bD.lo <= bD.hi ? static_cast<uint32_t>(bD.hi - bD.lo + 1) : 0;
+        const uint32_t wM = bM.lo <= bM.hi ? static_cast<uint32_t>(bM.hi - bM.lo + 1) : 0;
+        bI.base = used;
+        bD.base = used + wI;
+        bM.base = used + wI + wD;
+        if (!fits(static_cast<uint64_t>(used) + wI + wD + wM, s + 1)) {
+            overflow = true;
+            break;
+        }
+        used += wI + wD + wM;
+        int best_end_k = INT32_MAX, best_end_layer = 0;
+        for (int k = bM.lo + tid; k <= bM.hi; k += nthr) {
+            int32_t ins = UNSET, del = UNSET;
+            if (k >= bI.lo && k <= bI.hi) {
+                int32_t best = UNSET, iop = 0;
+                if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
+                    const int32_t c = vals[sMo.base + (k - 1 - sMo.lo)] + 1;
+                    if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 0; }
+                }
+                if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
+                    const int32_t c = vals[sIe.base + (k - 1 - sIe.lo)] + 1;
+                    if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 1; }
+                }
+                ins = best;
+                vals[bI.base + (k - bI.lo)] = ins;
+                auxs[bI.base + (k - bI.lo)] = static_cast<uint32_t>(iop);
+            }
+            if (k >= bD.lo && k <= bD.hi) {
+                int32_t best = UNSET, dop = 0;
+                if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
+                    const int32_t c = vals[sMo.base + (k + 1 - sMo.lo)];
+                    if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 0; }
+                }
+                if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
+                    const int32_t c = vals[sDe.base + (k + 1 - sDe.lo)];
+                    if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 1; }
+                }
+                del = best;
+                vals[bD.base + (k - bD.lo)] = del;
+                auxs[bD.base + (k - bD.lo)] = static_cast<uint32_t>(dop);
+            }
+            int32_t best = UNSET;
+            uint32_t mop = 0;
+            if (k >= sMx.lo && k <= sMx.hi) {
+                const int32_t c = vals[sMx.base + (k - sMx.lo)] + 1;
+                if (pos_ok(c, k, qn, tn)) { best = c; mop = 0; }
+            }
+            if (pos_ok(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
+            if (pos_ok(del, k, qn, tn) && del > best) { best = del; mop = 2; }
+            int32_t mval = UNSET;
+            uint32_t aux = 0;
+            if (best != UNSET) {
+                mval = extend_valid<S>(qb, qn, tb, tn, best, k, lcp_words);
+                aux = (static_cast<uint32_t>(best) << 2) | mop;
+            }
+            vals[bM.base + (k - bM.lo)] = mval;
+            auxs[bM.base + (k - bM.lo)] = aux;
+            const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
+            if (layer >= 0) {
+                if (!fitting) {
+                    if (k == qn - tn) { best_end_k = k; best_end_layer = layer; }
+                } else if (k >= qn - tn && k < best_end_k) {
+                    best_end_k = k;
+                    best_end_layer = layer;
+                }
+            }
+        }
+        if (tid == 0) {
+            AffDir e;
+            e.L[0] = LayerBand{bM.lo, bM.hi, bM.base};
+            e.L[1] = LayerBand{bI.lo, bI.hi, bI.base};
+            e.L[2] = LayerBand{bD.lo, bD.hi, bD.base};
+            dir_at(s) = e;
+        }
+        // CTA min over (k, layer): smallest k wins (largest t_end); one key per thread
+        const long long key = best_end_k == INT32_MAX
+                                  ? LLONG_MAX
+                                  : static_cast<long long>(best_end_k) * 4 + best_end_layer;  // layer < 4
+        long long wkey = key;
+        for (int o = 16; o > 0; o >>= 1) wkey = min(wkey, __shfl_xor_sync(PHR_FULL_MASK, wkey, o));
+        long long* red = reinterpret_cast<long long*>(sh_red);
+        if ((tid & 31) == 0) red[tid >> 5] = wkey;
+        __syncthreads();  // this score's cells, directory entry and partial minima are visible
+        long long best = LLONG_MAX;
+        for (int w = 0; w < nthr / 32; ++w) best = min(best, red[w]);
+        __syncthreads();  // `red` is rewritten by the next score
+        if (best != LLONG_MAX) {
+            done = true;
+            s_end = static_cast<int>(s);
+            k_end = static_cast<int>(best >> 2);   // floor(best / 4), also for negative k
+            layer_end = static_cast<int>(best & 3);
+            t_end = qn - k_end;
+        }
+        s += step;
+    }
+    if (P.work) {
+        if (tid == 0) atomicAdd(P.work + 2, static_cast<unsigned long long>(wf_cells));
+        if (lcp_words) atomicAdd(P.work + 3, static_cast<unsigned long long>(lcp_words));
+    }
+    const bool failed = !done && !overflow;
+    if (overflow && tid == 0) {
+        const uint64_t full = runs_bytes + 4ull * static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
+                              static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull + 4096;
+        const uint64_t grow = runs_bytes + 4ull * (static_cast<uint64_t>(used) * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) +
+                              4096;
+        report_redo(P, pid, min(full, grow));
+    }
+    __syncthreads();
+    if (tid < 32)
+        affine_finish(P, pid, true, 32, qn, tn, X, O, E, runs, auxs, dir_top, done, failed, s_end, t_end, k_end,
+                      layer_end);
+    __syncthreads();
+}
+
+template <class S>
+__global__ void __launch_bounds__(kBigThreads, 2) wfa_affine_big_kernel(ExtendParams P) {
+    extern __shared__ __align__(16) uint32_t big_sm[];
+    __shared__ uint32_t sh_task;
+    __shared__ __align__(8) long long sh_red[kBigThreads / 32];
+    __shared__ __align__(8) uint64_t sh_bar;
+    uint32_t phase = 0;  // parity of sh_bar's current phase, the same in every thread
+    if (threadIdx.x == 0) mbar_init(&sh_bar, 1);
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) sh_task = P.tasks.range[0] + atomicAdd(P.queue_head, 1u);
+        __syncthreads();
+        const uint32_t task = sh_task;
+        __syncthreads();
+        if (task >= P.tasks.range[1]) break;
+        if (!(P.tasks.task_group[task] & kBigTask)) continue;
+        const uint32_t pid = P.tasks.order[P.tasks.task_first[task]];
+        const PairDesc d = P.desc[pid];
+        if (d.mode != (S::kBits == 2 ? 0 : 1)) continue;
+        wfa_affine_cta<S>(P, d, pid, P.scratch + P.task_off[task], P.task_len[task] & ~15ull, big_sm, &sh_bar, phase,
+                          reinterpret_cast<int*>(sh_red));
+    }
+}
+
+// ===========================================================================
 // Gap-affine WFA, one pair per warp, wavefronts in registers
 // ===========================================================================
 // Every reachable cell of score s lies on a diagonal |k| <= (s - O) / E (a gap of length
@@ -1353,7 +1620,7 @@ __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams 
         uint8_t* slot = P.task_off ? P.scratch + P.task_off[task] : P.scratch + warp_global * P.slot_bytes;
         const uint64_t slot_bytes = P.task_off ? P.task_len[task] : P.slot_bytes;
         const uint8_t tg = P.tasks.task_group[task];
-        if (tg & kBigTask) continue;  // a redo task of wfa_linear_big_kernel
+        if (tg & kBigTask) continue;  // a redo task of a CTA-per-pair kernel
         const int G = tg;
         const int count = P.tasks.task_count[task];
         const int grp = lane / G;
@@ -1363,10 +1630,10 @@ __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams 
         if (act) d = P.desc[pid];
         // pairs of the other symbol mode run in the other instantiation
         act = act && d.mode == (S::kBits == 2 ? 0 : 1);
-        // long linear pairs run one per CTA: deferred from the main pass to the redo
-        // passes, where wfa_linear_big_kernel takes them
-        if (!kAffine && act && !P.task_off && big_pair(P.engine, P.big_min, P.big_smem, d.qn, d.tn, d.mode)) {
-            if ((lane & (G - 1)) == 0) report_redo(P, pid, wfa_region_est(d.qn, d.tn, false));
+        // long pairs run one per CTA: deferred from the main pass to the redo passes,
+        // where wfa_linear_big_kernel / wfa_affine_big_kernel take them
+        if (act && !P.task_off && big_pair(P.engine, P.big_min, P.big_smem, d.qn, d.tn, d.mode)) {
+            if ((lane & (G - 1)) == 0) report_redo(P, pid, wfa_region_est(d.qn, d.tn, kAffine));
             act = false;
         }
         if (!__any_sync(PHR_FULL_MASK, act)) continue;
@@ -1427,6 +1694,18 @@ void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream
         wfa_linear_big_kernel<SeqB><<<grid, kBigThreads, p.big_smem, st>>>(p);
     }
 }
+void launch_wfa_affine_big(const ExtendParams& p, int grid, int mode, cudaStream_t st) {
+    if (mode == 0) {
+        cudaFuncSetAttribute(wfa_affine_big_kernel<Seq2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(p.big_smem));
+        wfa_affine_big_kernel<Seq2><<<grid, kBigThreads, p.big_smem, st>>>(p);
+    } else {
+        cudaFuncSetAttribute(wfa_affine_big_kernel<SeqB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(p.big_smem));
+        wfa_affine_big_kernel<SeqB><<<grid, kBigThreads, p.big_smem, st>>>(p);
+    }
+}
+
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st) {
     const int smem = (block / 32) * kAffWarpSmem;
     cudaFuncSetAttribute(wfa_kernel<Seq2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -190,6 +190,41 @@ def test_long_linear_pairs_cta_kernel(eng):
         compare(e2, A.ENGINE_WFA_LINEAR, pairs)
 
 
+def long_affine_pairs():
+    """Gap-affine pairs long enough for the CTA-per-pair affine kernel (qlen+tlen >= 4096):
+    global and fitting branches, seed offsets, the byte path."""
+    rng = np.random.default_rng(22)
+    packed = D.extension_pairs(10, 2100, 4000, 0.06, seed=22)
+    pairs = [(bytes(packed.seq[packed.q_off[i]:packed.q_off[i] + packed.q_len[i]]),
+              bytes(packed.seq[packed.t_off[i]:packed.t_off[i] + packed.t_len[i]])) for i in range(packed.n)]
+    for i in range(4):  # fitting branch: read inside a window more than 1.5x its length
+        t = bytes(rng.choice(list(b"ACGT"), 6000).tolist())
+        s = int(rng.integers(0, 2000))
+        q = bytearray(t[s:s + 2200])
+        for _ in range(int(rng.integers(0, 60))):
+            q[int(rng.integers(0, len(q)))] = int(rng.choice(list(b"ACGT")))
+        pairs.append((bytes(q), t, 0, s if i % 2 else 0))
+    q = bytes(rng.choice(list(b"ACGT"), 3000).tolist())
+    pairs.append((q, q))                                     # identical
+    qb = bytearray(q)
+    for p in rng.integers(0, 3000, 30):
+        qb[int(p)] = ord("N")
+    pairs.append((bytes(qb), q.lower()[:2900] + q[2900:]))   # byte path
+    return pairs
+
+
+@pytest.mark.parametrize("costs", [(2, 4, 1), (4, 6, 2)])
+def test_long_affine_pairs_cta_kernel(costs):
+    pairs = long_affine_pairs()
+    with P.Engine(0) as e:
+        e.set_timing(True)
+        compare(e, A.ENGINE_WFA_AFFINE, pairs, costs)
+        assert e.kernel_times().get("wfa_affine_big", (0, 0.0))[0] >= 1
+        # CTA kernel off: the warp-group kernel on the same pairs
+        e.set_tune("wfa_big_min", 0)
+        compare(e, A.ENGINE_WFA_AFFINE, pairs, costs)
+
+
 def test_tune_keys_validated(eng):
     with pytest.raises(P.EngineError):
         eng.set_tune("no_such_key", 1)
