@@ -409,12 +409,13 @@ __device__ __forceinline__ uint32_t window_sm(const uint32_t* base, int32_t pos)
 
 template <class S>
 __device__ __forceinline__ int32_t extend_sm(const uint32_t* q, int32_t qn, const uint32_t* t, int32_t tn,
-                                             int32_t q_pos, int32_t k) {
+                                             int32_t q_pos, int32_t k, uint32_t& words) {
     const int32_t j = q_pos - k;
     if (q_pos < 0 || q_pos >= qn || j < 0 || j >= tn) return q_pos;
     const int32_t lim = min(qn - q_pos, tn - j);
     int32_t n = 0;
     while (n < lim) {
+        ++words;
         const uint32_t x = window_sm<S>(q, q_pos + n) ^ window_sm<S>(t, j + n);
         if (x != 0) {
             n += (__ffs(x) - 1) / S::kBits;
@@ -499,13 +500,15 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
     if (tid < 3) sh_end[tid] = INT32_MAX;
     const int max_s = qn + tn;
     bool done = false, overflow = false;
+    uint64_t wf_cells = 0;   // band diagonals of the scores computed
+    uint32_t lcp_words = 0;  // this thread's word compares of match extension
     int s_end = 0, t_end = 0, s = 1;
     if (lin_base(1, qn, tn) > cell_cap) overflow = true;
     if (fcap < 1) global_frames = true;
     __syncthreads();
     if (!overflow) {
         if (tid == 0) {
-            frame(0)[0] = extend_sm<S>(sq, qn, st, tn, 0, 0);
+            frame(0)[0] = extend_sm<S>(sq, qn, st, tn, 0, 0, lcp_words);
             hr[0] = 0;
         }
         __syncthreads();
@@ -528,6 +531,7 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
                 overflow = true;
                 break;
             }
+            wf_cells += static_cast<uint64_t>(width);
             if (!global_frames && static_cast<uint32_t>(width) > fcap) {
                 // frames outgrow shared memory: continue on the region's global frames
                 const int32_t* src = frame(s - 1);
@@ -579,7 +583,7 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
                 if (have) {
                     const int32_t j = best_pos - k;
                     if (!(best_pos < 0 || best_pos > qn || j < 0 || j > tn)) {
-                        val = extend_sm<S>(sq, qn, st, tn, best_pos, k);
+                        val = extend_sm<S>(sq, qn, st, tn, best_pos, k, lcp_words);
                         aux = (static_cast<uint32_t>(best_pos) << 2) | best_op;
                     }
                 }
@@ -605,6 +609,10 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
         }
     }
     if (done && s_end == 0) s = 0;
+    if (P.work) {  // work counters: band diagonals (the same in every thread), LCP word compares
+        if (tid == 0) atomicAdd(P.work + 2, static_cast<unsigned long long>(wf_cells));
+        if (lcp_words) atomicAdd(P.work + 3, static_cast<unsigned long long>(lcp_words));
+    }
     const bool failed = !done && !overflow;
     if (overflow && tid == 0) {
         const int64_t s2 = ::min(static_cast<long long>(max_s) + 1, 2LL * s + 64);
