@@ -1410,21 +1410,17 @@ __host__ __device__ constexpr int reg_slot_lo(int h) { return h == 0 ? -16 : h =
 __host__ __device__ constexpr int reg_left(int h) { return h == 0 ? 1 : h == 1 ? 3 : h == 2 ? 0 : h == 4 ? 2 : -1; }
 __host__ __device__ constexpr int reg_right(int h) { return h == 0 ? 2 : h == 1 ? 0 : h == 2 ? 4 : h == 3 ? 1 : -1; }
 
-// value at diagonal k - 1 (UP) or k + 1 of slot h, across lanes and into the adjacent slot;
-// a slot the band has never reached holds only UNSET, so its shuffle is skipped
-// (`active` is warp-uniform)
+// value at diagonal k - 1 (UP) or k + 1 of slot h, across lanes and into the adjacent slot
 template <bool UP>
-__device__ __forceinline__ int32_t reg_neighbor(const int32_t (&v)[kRegSlots], int h, uint32_t active) {
+__device__ __forceinline__ int32_t reg_neighbor(const int32_t (&v)[kRegSlots], int h) {
     const int lane = lane_id();
     if (UP) {
         const int32_t a = __shfl_up_sync(PHR_FULL_MASK, v[h], 1);
-        const int nb = reg_left(h);
-        const int32_t b = (nb >= 0 && ((active >> nb) & 1u)) ? __shfl_sync(PHR_FULL_MASK, v[nb], 31) : UNSET;
+        const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_left(h) >= 0 ? v[reg_left(h)] : UNSET, 31);
         return lane == 0 ? b : a;
     }
     const int32_t a = __shfl_down_sync(PHR_FULL_MASK, v[h], 1);
-    const int nb = reg_right(h);
-    const int32_t b = (nb >= 0 && ((active >> nb) & 1u)) ? __shfl_sync(PHR_FULL_MASK, v[nb], 0) : UNSET;
+    const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_right(h) >= 0 ? v[reg_right(h)] : UNSET, 0);
     return lane == 31 ? b : a;
 }
 
@@ -1516,10 +1512,10 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             const uint32_t vlo = vh >= vl ? static_cast<uint32_t>(vl) : 0x40000000u;
             const uint32_t vspan = vh >= vl ? static_cast<uint32_t>(vh - vl) : 0u;
             auto ok = [&](int32_t pos) { return static_cast<uint32_t>(pos) - vlo <= vspan; };
-            const int32_t mo_dn = reg_neighbor<true>(M[OES - 1], h, active);   // M[s - O - E][k - 1]
-            const int32_t ie_dn = reg_neighbor<true>(I[ES - 1], h, active);    // I[s - E][k - 1]
-            const int32_t mo_up = reg_neighbor<false>(M[OES - 1], h, active);  // M[s - O - E][k + 1]
-            const int32_t de_up = reg_neighbor<false>(D[ES - 1], h, active);   // D[s - E][k + 1]
+            const int32_t mo_dn = reg_neighbor<true>(M[OES - 1], h);   // M[s - O - E][k - 1]
+            const int32_t ie_dn = reg_neighbor<true>(I[ES - 1], h);    // I[s - E][k - 1]
+            const int32_t mo_up = reg_neighbor<false>(M[OES - 1], h);  // M[s - O - E][k + 1]
+            const int32_t de_up = reg_neighbor<false>(D[ES - 1], h);   // D[s - E][k + 1]
             // I (wfa_simd.rs:682-738): [open from M, extend I], strict >
             int32_t ins = UNSET;
             uint32_t iop = 0;
