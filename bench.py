@@ -180,7 +180,7 @@ def roofline(name, step_ms, launches, work, set_a, set_b, int_peak, hbm_peak, pe
     if traffic_gb is not None:
         traffic, traffic_src = traffic_gb * 1e9, "--traffic-gb-per-step"
     elif name == "myers_lane":
-        per_pair, traffic_src = traffic_record("myers_lane")
+        per_pair, traffic_src = traffic_record("myers_lane_ck" if ckpt else "myers_lane")
         traffic = per_pair * set_b.n if per_pair is not None else None
     out = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
            "traffic": traffic, "traffic_source": traffic_src, "kernel": name, "kernel_ms_per_step": step_ms,
