@@ -63,11 +63,17 @@ __host__ __device__ __forceinline__ uint64_t big_seq_words(int qn, int tn, int m
 }
 
 // A WFA pair (linear or gap-affine) long enough that one warp would be latency-bound on
-// it, whose sequences fit the CTA's shared memory with room for (linear) frames.
+// it: it runs one per CTA.
 __host__ __device__ __forceinline__ bool big_pair(int32_t engine, int32_t big_min, uint32_t big_smem, int qn, int tn,
                                                   int mode) {
-    if (big_min <= 0 || (engine != PHR_ENGINE_WFA_LINEAR && engine != PHR_ENGINE_WFA_AFFINE) || qn + tn < big_min)
-        return false;
+    (void)big_smem;
+    (void)mode;
+    return big_min > 0 && (engine == PHR_ENGINE_WFA_LINEAR || engine == PHR_ENGINE_WFA_AFFINE) && qn + tn >= big_min;
+}
+
+// Whether the CTA kernel stages a big pair's sequences in its shared memory (with room
+// left for the linear kernel's first frames); longer ones are read from global memory.
+__host__ __device__ __forceinline__ bool big_staged(uint32_t big_smem, int qn, int tn, int mode) {
     return (big_seq_words(qn, tn, mode) + 2ull * kBigMinFrameCells) * 4 <= big_smem;
 }
 

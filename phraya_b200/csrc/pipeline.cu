@@ -68,61 +68,140 @@ __device__ __forceinline__ uint64_t find_seq(const uint64_t* base, uint64_t n, u
     return lo;
 }
 
+constexpr int kSketchRun = 8;  // consecutive k-mer positions (windows) per thread, rolled
+
+__device__ __forceinline__ uint32_t nt_seed(uint32_t c) {
+    return c < 2u ? (c ? c_nt_seed[1] : c_nt_seed[0]) : (c == 2u ? c_nt_seed[2] : c_nt_seed[3]);
+}
+__device__ __forceinline__ uint32_t rotl32(uint32_t x, int r) { return __funnelshift_l(x, x, r & 31); }
+
 // Order hash of every k-mer: 32-bit ntHash over 2-bit codes, canonical = min(forward,
-// reverse complement) for DNA, forward for protein.
+// reverse complement) for DNA, forward for protein. A thread takes kSketchRun consecutive
+// positions: the first of a sequence is hashed whole, the next ones rolled,
+//   f(p + 1) = rotl(f(p), 1) ^ rotl(seed[c_p], k) ^ seed[c_{p+k}]
+//   r(p + 1) = rotr(r(p) ^ seed[~c_p], 1) ^ rotl(seed[~c_{p+k}], k - 1)
+// (XOR and rotations are exact, so the rolled hash equals the direct one). The four
+// seeds are picked by selects from uniform constant reads: an index per lane would
+// serialise the constant cache.
 __global__ void sketch_key_kernel(SketchArgs A) {
-    for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_k;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t s = find_seq(A.kbase, A.n, g);
-        const uint64_t p = g - A.kbase[s];
-        const uint8_t* b = A.seq + A.off[s] + p;
+    const uint64_t runs = (A.total_k + kSketchRun - 1) / kSketchRun;
+    const int k = A.k;
+    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < runs;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t g0 = r * kSketchRun;
+        const uint64_t g1 = g0 + kSketchRun < A.total_k ? g0 + kSketchRun : A.total_k;
+        uint64_t s = find_seq(A.kbase, A.n, g0);
+        uint64_t s_end = A.kbase[s + 1];
         uint32_t hf = 0, hr = 0;
-        for (int i = 0; i < A.k; ++i) {
-            const uint32_t c = (b[i] >> 1) & 3u;
-            hf ^= __funnelshift_l(c_nt_seed[c], c_nt_seed[c], (A.k - 1 - i) & 31);
-            hr ^= __funnelshift_l(c_nt_seed[c ^ 2u], c_nt_seed[c ^ 2u], i & 31);
+        bool fresh = true;
+        for (uint64_t g = g0; g < g1; ++g) {
+            while (g >= s_end) {  // next sequence (skipping those shorter than k)
+                ++s;
+                s_end = A.kbase[s + 1];
+                fresh = true;
+            }
+            const uint8_t* b = A.seq + A.off[s] + (g - A.kbase[s]);
+            if (fresh) {
+                hf = hr = 0;
+                for (int i = 0; i < k; ++i) {
+                    const uint32_t c = (b[i] >> 1) & 3u;
+                    hf ^= rotl32(nt_seed(c), k - 1 - i);
+                    hr ^= rotl32(nt_seed(c ^ 2u), i);
+                }
+                fresh = false;
+            } else {
+                const uint32_t co = (b[-1] >> 1) & 3u, ci = (b[k - 1] >> 1) & 3u;
+                hf = rotl32(hf, 1) ^ rotl32(nt_seed(co), k) ^ nt_seed(ci);
+                hr = rotl32(hr ^ nt_seed(co ^ 2u), 31) ^ rotl32(nt_seed(ci ^ 2u), k - 1);
+            }
+            A.key[g] = (A.alphabet == PHR_ALPHABET_DNA && hr < hf) ? hr : hf;
         }
-        A.key[g] = (A.alphabet == PHR_ALPHABET_DNA && hr < hf) ? hr : hf;
     }
 }
 
 // Selected k-mer of every window: the leftmost minimum hash, or for canonical (DNA)
 // minimizers the rightmost one when the window's l = w + k - 1 characters hold no more
-// T/G (codes 2, 3) than A/C.
+// T/G (codes 2, 3) than A/C. And flag = the window selects another k-mer than the
+// window before it (first window of a sequence: 1), so each selected k-mer is emitted
+// once per run of windows.
+// A thread takes kSketchRun consecutive windows of one sequence (plus the window before
+// the first, for its flag): the T/G count rolls by one character per window, and the
+// leftmost and rightmost positions of the window minimum roll by one key unless one of
+// them leaves the window, when the window is scanned again.
 __global__ void sketch_window_kernel(SketchArgs A) {
     const int l = A.w + A.k - 1;
-    for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_w;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t s = find_seq(A.wbase, A.n, g);
-        const uint64_t p = g - A.wbase[s];
-        const uint64_t* kk = A.key + A.kbase[s];
-        bool forward = true;
-        if (A.alphabet == PHR_ALPHABET_DNA) {
-            const uint8_t* b = A.seq + A.off[s] + p;
-            int tg = 0;
-            for (int i = 0; i < l; ++i) tg += (b[i] >> 2) & 1;  // bit 1 of the code (b >> 1) & 3
-            forward = 2 * tg > l;
-        }
-        uint64_t best = p;
-        uint64_t bk = kk[p];
-        for (uint64_t q = p + 1; q < p + A.w; ++q) {
-            const uint64_t v = kk[q];
-            if (v < bk || (!forward && v == bk)) {
-                best = q;
-                bk = v;
+    const int w = A.w;
+    const bool dna = A.alphabet == PHR_ALPHABET_DNA;
+    const uint64_t runs = (A.total_w + kSketchRun - 1) / kSketchRun;
+    for (uint64_t r = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; r < runs;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t g0 = r * kSketchRun;
+        const uint64_t g1 = g0 + kSketchRun < A.total_w ? g0 + kSketchRun : A.total_w;
+        uint64_t s = find_seq(A.wbase, A.n, g0);
+        uint64_t s_end = A.wbase[s + 1];
+        const uint8_t* bs = nullptr;
+        const uint64_t* kk = nullptr;
+        int tg = 0;
+        uint64_t lm = 0, rm = 0, bk = 0;  // leftmost / rightmost position of the window minimum, its key
+        uint32_t prev = 0;
+        auto scan_min = [&](uint64_t p) {  // minimum of window p from scratch
+            lm = rm = p;
+            bk = kk[p];
+            for (uint64_t q = p + 1; q < p + w; ++q) {
+                const uint64_t v = kk[q];
+                if (v < bk) {
+                    lm = rm = q;
+                    bk = v;
+                } else if (v == bk) {
+                    rm = q;
+                }
             }
+        };
+        auto roll = [&](uint64_t p) {  // window p from window p - 1
+            if (dna) tg += static_cast<int>((bs[p + l - 1] >> 2) & 1) - static_cast<int>((bs[p - 1] >> 2) & 1);
+            if (lm < p) {  // the leftmost minimum left the window (lm <= rm)
+                scan_min(p);
+                return;
+            }
+            const uint64_t v = kk[p + w - 1];
+            if (v < bk) {
+                lm = rm = p + w - 1;
+                bk = v;
+            } else if (v == bk) {
+                rm = p + w - 1;
+            }
+        };
+        auto pick = [&]() { return static_cast<uint32_t>((!dna || 2 * tg > l) ? lm : rm); };
+        bool fresh = true;
+        for (uint64_t g = g0; g < g1; ++g) {
+            while (g >= s_end) {  // next sequence (skipping those without a window)
+                ++s;
+                s_end = A.wbase[s + 1];
+                fresh = true;
+            }
+            const uint64_t p = g - A.wbase[s];
+            if (fresh) {
+                bs = A.seq + A.off[s];
+                kk = A.key + A.kbase[s];
+                // start at the window before the run (for this window's flag) if there is one
+                const uint64_t p0 = p > 0 ? p - 1 : 0;
+                tg = 0;
+                if (dna)
+                    for (int i = 0; i < l; ++i) tg += (bs[p0 + i] >> 2) & 1;  // bit 1 of the code (b >> 1) & 3
+                scan_min(p0);
+                if (p > 0) {
+                    prev = pick();
+                    roll(p);
+                }
+                fresh = false;
+            } else {
+                roll(p);
+            }
+            const uint32_t sel = pick();
+            A.sel[g] = sel;
+            A.flag[g] = (p == 0 || sel != prev) ? 1u : 0u;
+            prev = sel;
         }
-        A.sel[g] = static_cast<uint32_t>(best);
-    }
-}
-
-// flag = the window selects another k-mer than the window before it (first window of a
-// sequence: 1), so each selected k-mer is emitted once per run of windows.
-__global__ void sketch_flag_kernel(SketchArgs A) {
-    for (uint64_t g = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; g < A.total_w;
-         g += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t s = find_seq(A.wbase, A.n, g);
-        A.flag[g] = (g == A.wbase[s] || A.sel[g] != A.sel[g - 1]) ? 1u : 0u;
     }
 }
 
@@ -1149,18 +1228,21 @@ phr_status sketch_device(Ctx* ctx, DeviceArena& A, const uint8_t* seq, const uin
     O.remap_off = remap_off;
     const unsigned grid = std::max<unsigned>(1, std::min<unsigned>(blocks_for(std::max<uint64_t>(TK, 1), T),
                                                                     static_cast<unsigned>(ctx->sm_count * 16)));
+    // the key and window kernels take kSketchRun positions per thread
+    const auto run_grid = [&](uint64_t total) {
+        return std::max<unsigned>(1, std::min<unsigned>(blocks_for(std::max<uint64_t>((total + kSketchRun - 1) /
+                                                                                      kSketchRun, 1), T),
+                                                        static_cast<unsigned>(ctx->sm_count * 16)));
+    };
+    const unsigned grid_w = run_grid(TW);
     if (TK) {
         KernelScope ks(ctx, "sketch_key");
-        sketch_key_kernel<<<grid, T, 0, st>>>(S);
+        sketch_key_kernel<<<run_grid(TK), T, 0, st>>>(S);
     }
     if (TW) {
         {
             KernelScope ks(ctx, "sketch_window");
-            sketch_window_kernel<<<grid, T, 0, st>>>(S);
-        }
-        {
-            KernelScope ks(ctx, "sketch_flag");
-            sketch_flag_kernel<<<grid, T, 0, st>>>(S);
+            sketch_window_kernel<<<grid_w, T, 0, st>>>(S);
         }
         size_t ts = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, ts, S.flag, scan, static_cast<int>(TW), st);

@@ -23,6 +23,8 @@
 // later scores) and the pre-extension candidate `raw` with its op code. In both
 // tracebacks the match-run start is exactly `raw` (linear: edit_start = pred_pos+1 for
 // ops 1/2 and pred_pos for op 3 == the winning candidate; affine: raw of each m_op).
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace phr {
@@ -431,13 +433,22 @@ __device__ __forceinline__ int32_t extend_sm(const uint32_t* q, int32_t qn, cons
 // sequence from the 16-byte boundary at or below its first word to the next 16-byte
 // boundary after its last (the arenas are 256-byte aligned and hold four padding words
 // after every sequence, so both ends stay inside them). Called by every thread of the
-// CTA; returns the first free word after the staged sequences (16-byte aligned).
+// CTA; returns the first free word after the staged sequences (16-byte aligned). A pair
+// too long for the shared memory (big_staged) is read in place: 0 is returned and the
+// output pointers are the global ones.
 template <class S>
 __device__ uint32_t stage_pair_cta(const ExtendParams& P, const PairDesc& d, uint32_t* sm, uint64_t* bar,
                                    uint32_t& phase, uint32_t** sq_out, uint32_t** st_out) {
     const int tid = threadIdx.x;
     const uint32_t* gq = seq_base<S>(P, d.q_word);
     const uint32_t* gt = seq_base<S>(P, d.t_word);
+    if (!big_staged(P.big_smem, d.qn, d.tn, S::kBits == 2 ? 0 : 1)) {
+        // too long for shared memory: read in place (each sequence is followed by padding
+        // words in its arena, and every match extension is clamped to the sequence ends)
+        *sq_out = const_cast<uint32_t*>(gq);
+        *st_out = const_cast<uint32_t*>(gt);
+        return 0;
+    }
     const int qw = (d.qn + S::kPerWord - 1) / S::kPerWord;
     const int tw = (d.tn + S::kPerWord - 1) / S::kPerWord;
     const int lead_q = static_cast<int>((reinterpret_cast<uintptr_t>(gq) & 15) >> 2);
@@ -757,12 +768,16 @@ __device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
 __device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int G, int qn, int tn, int X, int O,
                               int E, uint32_t* runs, const uint32_t* auxs, const AffDir* dir_top, bool done,
                               bool failed, int s_end, int t_end, int k_end, int layer_end, int row_g = 0,
-                              int row_w = 0, int row_lo = 0) {
+                              int row_w = 0, int row_lo = 0, const uint32_t* sh_hist = nullptr, int sh_rows = 0) {
     const int gl = lane_id() & (G - 1);
     auto dir_at = [&](int64_t sc) -> const AffDir& { return dir_top[-1 - sc]; };
     auto aux_at = [&](int ss, int layer, int k) -> uint32_t {
         if (row_g > 0) {
-            const uint32_t w = auxs[static_cast<uint64_t>(ss / row_g) * row_w + (k - row_lo)];
+            // rows below sh_rows of diagonals -16..15 live in shared memory
+            const int rr = ss / row_g;
+            const uint32_t w = (rr < sh_rows && static_cast<unsigned>(k + 16) < 32u)
+                                   ? sh_hist[rr * 32 + (k + 16)]
+                                   : auxs[static_cast<uint64_t>(rr) * row_w + (k - row_lo)];
             return layer == 0 ? (((w >> 4) << 2) | (w & 3u)) : (w >> (layer + 1)) & 1u;
         }
         const LayerBand& b = dir_at(ss).L[layer];
@@ -1410,23 +1425,30 @@ __host__ __device__ constexpr int reg_slot_lo(int h) { return h == 0 ? -16 : h =
 __host__ __device__ constexpr int reg_left(int h) { return h == 0 ? 1 : h == 1 ? 3 : h == 2 ? 0 : h == 4 ? 2 : -1; }
 __host__ __device__ constexpr int reg_right(int h) { return h == 0 ? 2 : h == 1 ? 0 : h == 2 ? 4 : h == 3 ? 1 : -1; }
 
-// value at diagonal k - 1 (UP) or k + 1 of slot h, across lanes and into the adjacent slot
-template <bool UP>
+// value at diagonal k - 1 (UP) or k + 1 of slot h, across lanes and into the adjacent slot;
+// SOLO: the band has never left slot h, so the adjacent slot holds UNSET everywhere
+template <bool UP, bool SOLO>
 __device__ __forceinline__ int32_t reg_neighbor(const int32_t (&v)[kRegSlots], int h) {
     const int lane = lane_id();
     if (UP) {
         const int32_t a = __shfl_up_sync(PHR_FULL_MASK, v[h], 1);
-        const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_left(h) >= 0 ? v[reg_left(h)] : UNSET, 31);
+        const int32_t b =
+            SOLO ? UNSET : __shfl_sync(PHR_FULL_MASK, reg_left(h) >= 0 ? v[reg_left(h)] : UNSET, 31);
         return lane == 0 ? b : a;
     }
     const int32_t a = __shfl_down_sync(PHR_FULL_MASK, v[h], 1);
-    const int32_t b = __shfl_sync(PHR_FULL_MASK, reg_right(h) >= 0 ? v[reg_right(h)] : UNSET, 0);
+    const int32_t b = SOLO ? UNSET : __shfl_sync(PHR_FULL_MASK, reg_right(h) >= 0 ? v[reg_right(h)] : UNSET, 0);
     return lane == 31 ? b : a;
 }
 
+// History rows of slot 0 (diagonals -16..15) kept in the warp's shared memory: rows of
+// scores 0 .. (kRegShRows - 1) g, which hold the whole history of most short pairs, so
+// their traceback reads shared memory.
+constexpr int kRegShRows = 32;
+
 template <class S, int XS, int OES, int ES>
 __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
-                               uint64_t region_bytes) {
+                               uint64_t region_bytes, uint32_t* sh_hist) {
     constexpr int RM = (XS > OES ? XS : OES);  // M values kept: steps 1..RM back
     const int lane = lane_id();
     const int qn = d.qn, tn = d.tn;
@@ -1466,7 +1488,7 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
     if (!overflow) {
         if (lane == 0) v0 = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
         v0 = __shfl_sync(PHR_FULL_MASK, v0, 0);
-        if (lane == 0) auxs[-kRegLo] = 0;  // row 0 = score 0, diagonal 0
+        if (lane == 0) sh_hist[16] = 0;  // row 0 = score 0, diagonal 0 (slot 0, lane 16)
         if (lane == 16) M[0][0] = v0;  // diagonal 0: slot 0, lane 16
         if (!fitting) {
             if (qn - tn == 0 && v0 == qn) done = true, t_end = tn;
@@ -1496,13 +1518,16 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
         }
         if (lane == 0) wf_cells += static_cast<uint32_t>(bhi - blo + 1);
         uint32_t* arow = auxs + row * kRegWin;
+        uint32_t* srow = row < kRegShRows ? sh_hist + row * 32 : nullptr;
         int32_t nM[kRegSlots], nI[kRegSlots], nD[kRegSlots];
         int best_k = INT32_MAX, best_l = 0;
-#pragma unroll
-        for (int h = 0; h < kRegSlots; ++h) {
+        // one slot of this score; h and SOLO are compile-time
+        auto step_slot = [&](auto hc, auto soloc) {
+            constexpr int h = decltype(hc)::value;
+            constexpr bool solo = decltype(soloc)::value;
             nM[h] = nI[h] = nD[h] = UNSET;
-            const int klo = reg_slot_lo(h);
-            if (klo + 31 < blo || klo > bhi) continue;  // warp-uniform: slot outside the band
+            constexpr int klo = reg_slot_lo(h);
+            if (klo + 31 < blo || klo > bhi) return;  // warp-uniform: slot outside the band
             active |= 1u << h;
             const int k = klo + lane;
             // affine_pos_valid for this diagonal as one unsigned range test: pos in
@@ -1512,10 +1537,10 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             const uint32_t vlo = vh >= vl ? static_cast<uint32_t>(vl) : 0x40000000u;
             const uint32_t vspan = vh >= vl ? static_cast<uint32_t>(vh - vl) : 0u;
             auto ok = [&](int32_t pos) { return static_cast<uint32_t>(pos) - vlo <= vspan; };
-            const int32_t mo_dn = reg_neighbor<true>(M[OES - 1], h);   // M[s - O - E][k - 1]
-            const int32_t ie_dn = reg_neighbor<true>(I[ES - 1], h);    // I[s - E][k - 1]
-            const int32_t mo_up = reg_neighbor<false>(M[OES - 1], h);  // M[s - O - E][k + 1]
-            const int32_t de_up = reg_neighbor<false>(D[ES - 1], h);   // D[s - E][k + 1]
+            const int32_t mo_dn = reg_neighbor<true, solo>(M[OES - 1], h);   // M[s - O - E][k - 1]
+            const int32_t ie_dn = reg_neighbor<true, solo>(I[ES - 1], h);    // I[s - E][k - 1]
+            const int32_t mo_up = reg_neighbor<false, solo>(M[OES - 1], h);  // M[s - O - E][k + 1]
+            const int32_t de_up = reg_neighbor<false, solo>(D[ES - 1], h);   // D[s - E][k + 1]
             // I (wfa_simd.rs:682-738): [open from M, extend I], strict >
             int32_t ins = UNSET;
             uint32_t iop = 0;
@@ -1553,7 +1578,10 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             nM[h] = mval;
             nI[h] = ins;
             nD[h] = del;
-            arow[k - kRegLo] = aux;
+            if (h == 0 && srow)
+                srow[lane] = aux;
+            else
+                arow[k - kRegLo] = aux;
             // end cell: value == qn in layer order m, ins, del; smallest k (largest t_end)
             const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
             const bool cand = layer >= 0 && (fitting ? k >= qn - tn : k == qn - tn);
@@ -1566,11 +1594,9 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
                     best_l = l;
                 }
             }
-        }
-        // shift the histories of the reached slots: this score becomes one step back
-#pragma unroll
-        for (int h = 0; h < kRegSlots; ++h) {
-            if (!((active >> h) & 1u)) continue;
+        };
+        // shift the history of slot h: this score becomes one step back
+        auto shift_slot = [&](int h) {
 #pragma unroll
             for (int r = RM - 1; r > 0; --r) M[r][h] = M[r - 1][h];
             M[0][h] = nM[h];
@@ -1581,6 +1607,21 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             }
             I[0][h] = nI[h];
             D[0][h] = nD[h];
+        };
+        if (blo >= -16 && bhi <= 15) {
+            // the band has never left slot 0 (it only grows): one slot, no cross-slot shuffles
+            step_slot(std::integral_constant<int, 0>{}, std::true_type{});
+            shift_slot(0);
+        } else {
+            step_slot(std::integral_constant<int, 0>{}, std::false_type{});
+            step_slot(std::integral_constant<int, 1>{}, std::false_type{});
+            step_slot(std::integral_constant<int, 2>{}, std::false_type{});
+            step_slot(std::integral_constant<int, 3>{}, std::false_type{});
+            step_slot(std::integral_constant<int, 4>{}, std::false_type{});
+            static_assert(kRegSlots == 5, "one step_slot call per slot");
+#pragma unroll
+            for (int h = 0; h < kRegSlots; ++h)
+                if ((active >> h) & 1u) shift_slot(h);
         }
         ++row;  // the traceback addresses row s / g directly (no directory)
         if (best_k != INT32_MAX) {
@@ -1605,11 +1646,12 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
     }
     __syncwarp();
     affine_finish(P, pid, true, 32, qn, tn, X, O, E, runs, auxs, nullptr, done, !done, s_end, t_end, k_end,
-                  layer_end, g, kRegWin, kRegLo);
+                  layer_end, g, kRegWin, kRegLo, sh_hist, kRegShRows);
 }
 
 // Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
-constexpr int kAffWarpSmem = kAffRingGroups * kAffRing * static_cast<int>(sizeof(SDir)) + kWarpSeqWords * 4;
+constexpr int kAffGroupSmem = kAffRingGroups * kAffRing * static_cast<int>(sizeof(SDir)) + kWarpSeqWords * 4;
+constexpr int kAffWarpSmem = kAffGroupSmem > kRegShRows * 128 ? kAffGroupSmem : kRegShRows * 128;
 
 template <class S, bool kAffine>
 __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams P) {
@@ -1654,12 +1696,14 @@ __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams 
             // wavefronts in registers (redo passes and wide bands take the group kernel)
             if (G == 32 && !P.task_off && act && d.qn + d.tn < kRegMaxLen) {
                 const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
+                uint32_t* sh_hist = reinterpret_cast<uint32_t*>(wfa_smem + static_cast<size_t>(threadIdx.x >> 5) *
+                                                                                  kAffWarpSmem);
                 if (X == 4 && O == 6 && E == 2) {
-                    wfa_affine_reg<S, 2, 4, 1>(P, d, pid, region, region_bytes);
+                    wfa_affine_reg<S, 2, 4, 1>(P, d, pid, region, region_bytes, sh_hist);
                     continue;
                 }
                 if (X == 2 && O == 4 && E == 1) {
-                    wfa_affine_reg<S, 2, 5, 1>(P, d, pid, region, region_bytes);
+                    wfa_affine_reg<S, 2, 5, 1>(P, d, pid, region, region_bytes, sh_hist);
                     continue;
                 }
             }

@@ -43,12 +43,14 @@ def test_roofline_fields(bench, sets):
         r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback", ckpt=ckpt)
         assert r["frac"] == pytest.approx(r["achieved"] / r["peak"])
     # traffic: from the capture record only when it was taken of the current kernel source
-    per, why = bench.traffic_record("myers_lane")
-    r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")
-    if per is None:
-        assert r["traffic"] is None and r["traffic_source"] == why
-    else:
-        assert r["traffic"] == pytest.approx(per * set_b.n)
+    # (the checkpointed and the record-mode kernels have records of their own)
+    for ckpt, key in ((1, "myers_lane_ck"), (0, "myers_lane")):
+        per, why = bench.traffic_record(key)
+        r = bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback", ckpt=ckpt)
+        if per is None:
+            assert r["traffic"] is None and r["traffic_source"] == why
+        else:
+            assert r["traffic"] == pytest.approx(per * set_b.n)
     assert bench.roofline("myers_lane", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback",
                           traffic_gb=2.0)["traffic"] == pytest.approx(2.0e9)
     assert bench.roofline("pack", 0.5, 1.0, work, set_a, set_b, int_peak, hbm_peak, "fallback")["bound"] is None
