@@ -4,8 +4,10 @@
 // phraya-cli/src/main.rs:583-590). Requests are single reads. A scheduler thread forms
 // batches continuously from two length buckets (short reads <= 500 bases ride the Myers
 // path, long ones the WFA path): it fills a batch from one bucket up to
-// max_batch_reads / max_batch_bases and hands it to an idle worker once the device has
-// the free memory the batch needs (cudaMemGetInfo minus the configured reserve).
+// max_batch_reads / max_batch_bases and hands it to an idle worker, which starts it once
+// the device has the free memory the batch needs (cudaMemGetInfo minus the configured
+// reserve). The scheduler itself makes no CUDA call, so nothing a worker waits on
+// delays the dispatch of other batches.
 //
 // Each worker owns a context (its own CUDA stream, device arenas and pinned host
 // buffers) and runs the whole align_read pipeline for its batch; workers overlap on the
@@ -216,6 +218,11 @@ void finish_batch(phr_server* S, phr_server::Worker* W, std::vector<Request>& ba
     S->cv_work.notify_all();
 }
 
+// Device bytes one batch may add to a worker's arenas (upper estimate).
+uint64_t batch_need(uint64_t n, uint64_t bases) {
+    return phr::align_arena_need(n, bases, 0) + bases * 64 + (64ull << 20);
+}
+
 void run_worker(phr_server* S, phr_server::Worker* W) {
     cudaSetDevice(W->ctx.device);
     for (;;) {
@@ -265,6 +272,23 @@ void run_worker(phr_server* S, phr_server::Worker* W) {
         rb.len = len;
         phr_read_result_arena ar{W->rr.as<phr_read_result>(), W->aln.as<phr_alignment>(), acap, 0,
                                  W->cig.as<char>(), cig_cap, 0};
+        if (!W->short_only) {
+            // admission by free HBM: wait while a batch this size does not fit and another
+            // worker may still free memory. The short lane skips it: its arenas were sized
+            // for a full short batch at creation.
+            const uint64_t need = batch_need(n, bases);
+            for (;;) {
+                size_t free_b = SIZE_MAX, total_b = 0;
+                cudaMemGetInfo(&free_b, &total_b);
+                if (free_b >= need + S->cfg.hbm_reserve_bytes) break;
+                std::unique_lock<std::mutex> lk(S->mu);
+                const bool others_busy = std::any_of(S->workers.begin(), S->workers.end(),
+                                                     [&](auto* w) { return w != W && w->busy; });
+                if (!others_busy || S->stopping) break;
+                const uint64_t seen = S->completions;
+                S->cv_work.wait(lk, [&] { return S->stopping || S->completions != seen; });
+            }
+        }
         const auto tb0 = Clock::now();
         const phr_status st = phr::align_reads_host(&W->ctx, S->idx, &rb, S->cfg.align, &ar, nullptr);
         if (S->trace) {
@@ -287,13 +311,8 @@ void run_worker(phr_server* S, phr_server::Worker* W) {
     }
 }
 
-// Device bytes one batch may add to a worker's arenas (upper estimate).
-uint64_t batch_need(uint64_t n, uint64_t bases) {
-    return phr::align_arena_need(n, bases, 0) + bases * 64 + (64ull << 20);
-}
 
 void run_scheduler(phr_server* S) {
-    cudaSetDevice(S->owner->device);
     std::unique_lock<std::mutex> lk(S->mu);
     // bucket an idle worker can take now: -1 none
     auto pick = [&](const phr_server::Worker* w) -> int {
@@ -342,25 +361,9 @@ void run_scheduler(phr_server* S) {
             batch.push_back(std::move(S->pending[b].front()));
             S->pending[b].pop_front();
         }
-        // admission by free HBM: wait while a batch this size does not fit. The short lane
-        // skips it: its arenas were sized for a full short batch at creation, and a query
-        // of free memory can wait on another worker's allocator work.
-        size_t free_b = SIZE_MAX, total_b = 0;
-        if (!W->short_only) {
-            lk.unlock();
-            cudaMemGetInfo(&free_b, &total_b);
-            lk.lock();
-        }
-        const uint64_t need = batch_need(batch.size(), bases);
-        const bool others_busy =
-            std::any_of(S->workers.begin(), S->workers.end(), [](auto* w) { return w->busy; });
-        if (!W->short_only && free_b < need + S->cfg.hbm_reserve_bytes && others_busy) {
-            // put the batch back (front, same order) and wait for a worker to finish
-            for (auto it = batch.rbegin(); it != batch.rend(); ++it) S->pending[b].push_front(std::move(*it));
-            const uint64_t seen = S->completions;
-            S->cv_work.wait(lk, [&] { return S->stopping || S->completions != seen; });
-            continue;
-        }
+        // (admission by free HBM happens in the worker: a query of free memory can take
+        // tens of milliseconds while other threads allocate, and this thread must keep
+        // handing short reads to the short lane meanwhile)
         W->batch = std::move(batch);
         W->busy = true;
         W->has_work = true;
