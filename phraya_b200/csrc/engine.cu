@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <unordered_set>
 
@@ -954,6 +955,21 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         std::vector<uint32_t> idx(h_redo);
         for (uint32_t i = 0; i < h_redo; ++i) idx[i] = i;
         std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return h_rneed[a] > h_rneed[b]; });
+        if (const char* tp = std::getenv("PHRAYA_EXTEND_TRACE")) {
+            // one line per redo round: engine round pairs budget, then the eight largest
+            // needs as qn:tn:need_bytes
+            if (FILE* f = std::fopen(tp, "a")) {
+                std::fprintf(f, "engine %d round %d pairs %u budget %llu", static_cast<int>(engine), round, h_redo,
+                             static_cast<unsigned long long>(ctx->scratch_budget));
+                for (uint32_t i = 0; i < std::min<uint32_t>(h_redo, 8); ++i) {
+                    PairDesc hd{};
+                    PHR_CUDA_TRY(ctx, cudaMemcpy(&hd, desc + h_list[idx[i]], sizeof(PairDesc), cudaMemcpyDeviceToHost));
+                    std::fprintf(f, " %d:%d:%llu", hd.qn, hd.tn, h_rneed[idx[i]]);
+                }
+                std::fprintf(f, "\n");
+                std::fclose(f);
+            }
+        }
         size_t pos = 0;
         while (pos < idx.size()) {
             std::vector<uint32_t> pl;
