@@ -125,7 +125,9 @@ void phr_ctx_destroy(phr_ctx* ctx);
 /* Launch parameters of the extension kernels. No counterpart in the reference (its
  * kernels are CPU code with nothing to tune); results never depend on them. Keys:
  *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen
- *                                        wfa_long_min (power of two, 1..32)
+ *                                        wfa_long_min (power of two, 1..32; short linear
+ *                                        pairs keep their wavefronts in registers with 16
+ *                                        or 32, the default)
  *   "wfa_affine_group_short"             lanes per gap-affine WFA pair below that edge
  *                                        (power of two, 1..32; "wfa_group_short" is then
  *                                        the linear engine's)
@@ -176,6 +178,9 @@ void phr_ctx_reset_timing(phr_ctx* ctx);
  * it handed to the every-block redo pass; "wfa_affine_cells" / "wfa_linear_cells" count
  * wavefront diagonals computed (the M band of each score) and "wfa_affine_lcp_words" /
  * "wfa_linear_lcp_words" the word compares of match extension. Unknown names read 0.
+ * With the environment variable PHRAYA_EXTEND_TRACE=<file> set, each redo round of an
+ * extension call appends one line to that file: engine, round, pairs, scratch budget
+ * and the eight largest scratch needs as qlen:tlen:bytes.
  */
 uint64_t phr_ctx_counter(const phr_ctx* ctx, const char* name);
 /* The cudaStream_t the context launches on (for callers that order their own work). */
