@@ -598,7 +598,12 @@ def _read_parity(gpu, oracle_rows, idx=None):
     bad = [j for j, i in enumerate(idx) if gpu[i] != oracle_rows[j]]
     out = {"reads": len(oracle_rows), "mismatches": len(bad)}
     if bad:
-        out["first_mismatch"] = int(list(idx)[bad[0]])
+        first = int(list(idx)[bad[0]])
+        out["first_mismatch"] = first
+
+        def brief(row):  # outcome, has_result, reverse, then (ed, qs, qe, ts, te, CIGAR length) per alignment
+            return [row[0], row[1], row[2], [[a[1], a[2], a[3], a[4], a[5], len(a[0])] for a in row[3]]]
+        out["first_mismatch_detail"] = {"gpu": brief(gpu[first]), "oracle": brief(oracle_rows[bad[0]])}
     return out
 
 

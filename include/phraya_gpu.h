@@ -125,9 +125,7 @@ void phr_ctx_destroy(phr_ctx* ctx);
 /* Launch parameters of the extension kernels. No counterpart in the reference (its
  * kernels are CPU code with nothing to tune); results never depend on them. Keys:
  *   "wfa_group_short", "wfa_group_long"  lanes per WFA pair below / from qlen+tlen
- *                                        wfa_long_min (power of two, 1..32; short linear
- *                                        pairs keep their wavefronts in registers with 16
- *                                        or 32, the default)
+ *                                        wfa_long_min (power of two, 1..32)
  *   "wfa_affine_group_short"             lanes per gap-affine WFA pair below that edge
  *                                        (power of two, 1..32; "wfa_group_short" is then
  *                                        the linear engine's)
@@ -135,17 +133,18 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *   "myers_band_base"                    Myers stored-band half-width base (>= 0)
  *   "block_threads"                      threads per block of the warp-per-pair kernels
  *                                        (32..256, multiple of 32)
- *   "wfa_big_min"                        linear WFA pairs with qlen+tlen >= this run one
- *                                        per CTA (0 = never)
- *   "wfa_big_smem"                       shared memory of that kernel, bytes (16 KiB..200 KiB)
+ *   "wfa_big_min"                        WFA pairs (linear and gap-affine) with qlen+tlen
+ *                                        >= this run one per CTA (0 = never)
+ *   "wfa_big_smem"                       shared memory of those kernels, bytes (16 KiB..200
+ *                                        KiB; longer pairs are read from global memory)
  *   "max_blocks_per_sm"                  resident blocks per SM of the persistent extension
  *                                        kernels (1..4)
  *   "host_chunks"                        chunks a host batch of more than 128 MiB of sequence
  *                                        is copied and aligned in, overlapped (2..32, default 4)
  *   "myers_lane_ckpt"                    banded Myers (global 2-bit pairs): 1 = keep the band's
  *                                        state every 4th column and recompute 4 columns at a
- *                                        time in shared memory for the traceback (default),
- *                                        0 = store every column's records
+ *                                        time for the traceback (default), 0 = store every
+ *                                        column's records
  * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune
  * file (written by the autotuner); unknown keys and bad values there are ignored. */
 phr_status phr_ctx_set_tune(phr_ctx* ctx, const char* key, int64_t value);
@@ -180,7 +179,8 @@ void phr_ctx_reset_timing(phr_ctx* ctx);
  * "wfa_linear_lcp_words" the word compares of match extension. Unknown names read 0.
  * With the environment variable PHRAYA_EXTEND_TRACE=<file> set, each redo round of an
  * extension call appends one line to that file: engine, round, pairs, scratch budget
- * and the eight largest scratch needs as qlen:tlen:bytes.
+ * and the eight largest scratch needs as qlen:tlen:bytes; and each call appends one line
+ * per pair of qlen + tlen >= 65536 with its final status and distance.
  */
 uint64_t phr_ctx_counter(const phr_ctx* ctx, const char* name);
 /* The cudaStream_t the context launches on (for callers that order their own work). */

@@ -1027,6 +1027,22 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
 
     hs_redo.stop();
     if (n_oom) ctx->counters["scratch_oom_pairs"] += n_oom;
+    if (const char* tp = std::getenv("PHRAYA_EXTEND_TRACE")) {
+        // one line per pair of qlen + tlen >= 65536: its final status and distance
+        std::vector<PairDesc> hd(n);
+        std::vector<PairOut> ho(n);
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(hd.data(), desc, n * sizeof(PairDesc), cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaMemcpyAsync(ho.data(), pout, n * sizeof(PairOut), cudaMemcpyDeviceToHost, st));
+        PHR_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        if (FILE* f = std::fopen(tp, "a")) {
+            for (uint64_t i = 0; i < n; ++i)
+                if (static_cast<int64_t>(hd[i].qn) + hd[i].tn >= 65536)
+                    std::fprintf(f, "engine %d pair %llu %d:%d seed %d:%d status %d ed %d\n", static_cast<int>(engine),
+                                 static_cast<unsigned long long>(i), hd[i].qn, hd[i].tn, hd[i].qs, hd[i].ts,
+                                 ho[i].status, ho[i].ed);
+            std::fclose(f);
+        }
+    }
     HostScope hs_tail(ctx, "host:extend_tail");
     // pack CIGAR text
     {

@@ -163,6 +163,15 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
     if (g.slide && P < nb) load_block_words(qb, P, qn);
     uint32_t tw = 0;
     uint32_t tw_next = n > 0 ? __ldg(tb) : 0u;
+    // 2-bit target symbol of column index jj (called for jj = 0, 1, 2, ... in order)
+    auto next_sym = [&](int jj) -> uint32_t {
+        if ((jj & 15) == 0) {
+            tw = tw_next;
+            const int nw = (jj >> 4) + 1;
+            tw_next = nw * 16 < n ? __ldg(tb + nw) : 0u;
+        }
+        return (tw >> ((jj & 15) * 2)) & 3u;
+    };
     uint8_t* r = rec + lane * (16 * kLaneColGroup);   // current column group of this lane
     for (int j = 1; j <= g.n_max; ++j) {
         if (j == next_shift) {  // warp-uniform: drop the top block, a new block enters
@@ -185,12 +194,7 @@ __device__ __forceinline__ void lane_forward(const uint32_t* __restrict__ qb, co
             next_shift += 64;
         }
         const int jj = j - 1;
-        if ((jj & 15) == 0) {
-            tw = tw_next;
-            const int nw = (jj >> 4) + 1;
-            tw_next = nw * 16 < n ? __ldg(tb + nw) : 0u;
-        }
-        const uint32_t c = (tw >> ((jj & 15) * 2)) & 3u;
+        const uint32_t c = next_sym(jj);
         const uint64_t* eqp = sp + c * 32 + lane;
         const int sub = jj % kLaneColGroup;
         uint32_t pa = 0, ma = 0;
@@ -400,6 +404,8 @@ __device__ __forceinline__ bool lane_trace_ck(const uint32_t* __restrict__ qb, c
     uint4* seg = reinterpret_cast<uint4*>(ck + lane_ckpt_bytes(g.n_max, P));
     int i = act ? m : 0, j = act ? n : 0, cost = 0;
     bool ok = act;
+    int q_idx = -1;       // query word held in q_word (the walk's row moves slowly)
+    uint32_t q_word = 0;
     if (g.n_max > 0) {
         const int S = (g.n_max - 1) / kSegCols;
         int ring_lo = lane_blo(g, S * kSegCols);  // the ring holds blocks [ring_lo, ring_lo + P]
@@ -483,7 +489,15 @@ __device__ __forceinline__ bool lane_trace_ck(const uint32_t* __restrict__ qb, c
                     j -= 1;
                     cost += 1;
                 } else {
-                    const uint32_t x = sym_at<Seq2>(qb, i - 1) != sym_at<Seq2>(tb, j - 1) ? 1u : 0u;
+                    // target symbol j - 1 from the segment's word; query word cached
+                    const int qwi = (i - 1) >> 4;
+                    if (qwi != q_idx) {
+                        q_idx = qwi;
+                        q_word = __ldg(qb + qwi);
+                    }
+                    const uint32_t qs = (q_word >> (((i - 1) & 15) * 2)) & 3u;
+                    const uint32_t ts = (tw >> (((j - 1) & 15) * 2)) & 3u;
+                    const uint32_t x = qs != ts ? 1u : 0u;
                     rw.push(x, 1);
                     cost += static_cast<int>(x);
                     i -= 1;

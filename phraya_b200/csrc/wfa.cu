@@ -625,9 +625,34 @@ __device__ void wfa_linear_cta(const ExtendParams& P, const PairDesc& d, uint32_
         if (lcp_words) atomicAdd(P.work + 3, static_cast<unsigned long long>(lcp_words));
     }
     const bool failed = !done && !overflow;
-    if (overflow && tid == 0) {
-        const int64_t s2 = ::min(static_cast<long long>(max_s) + 1, 2LL * s + 64);
-        report_redo(P, pid, fixed + lin_base(s2, qn, tn) * 4 + 64);
+    if (overflow) {  // CTA-uniform
+        // Scratch for the redo: extrapolate the final score from the progress so far (the
+        // furthest query offset the last score reached; the wavefront advances about in
+        // proportion to the score), plus a quarter as margin, so that one redo usually
+        // suffices; at least twice the scores reached, at most the whole search.
+        int vm = 0;
+        if (s >= 2) {
+            const int32_t* pf = frame(s - 1);
+            const int plo = -min(s - 1, tn), phi = min(s - 1, qn);
+            for (int k = plo + tid; k <= phi; k += nthr) vm = max(vm, pf[k - plo]);
+        }
+        vm = __reduce_max_sync(PHR_FULL_MASK, vm);
+        __syncthreads();  // every thread is done with the end flags
+        if (tid == 0) sh_end[0] = 0;
+        __syncthreads();
+        if ((tid & 31) == 0) atomicMax(&sh_end[0], vm);
+        __syncthreads();
+        if (tid == 0) {
+            const int64_t reach = sh_end[0];
+            int64_t s2 = 2LL * s + 64;
+            if (reach > 0) {
+                int64_t est = static_cast<int64_t>(s) * qn / reach;
+                est += est / 4 + 64;
+                s2 = ::max(s2, est);
+            }
+            s2 = ::min(static_cast<int64_t>(max_s) + 1, s2);
+            report_redo(P, pid, fixed + lin_base(s2, qn, tn) * 4 + 64);
+        }
     }
 
     // ---- traceback (wfa_simd.rs:959-1041) by thread 0, formatting by warp 0 ----
@@ -764,14 +789,23 @@ __device__ __forceinline__ bool pos_ok(int32_t pos, int k, int qn, int tn) {
 // the warp; the leader of each group of G lanes walks its pair.
 // With row_g > 0 the history is the register kernel's: one word per (score, k) at
 // auxs[(score / row_g) * row_w + k - row_lo] holding raw << 4 | dop << 3 | iop << 2 | mop
-// (all three layers' history of the cell), no directory read.
+// (all three layers' history of the cell), no directory read. With `folded` the same
+// words are laid out per score over its M band, found through the directory (the CTA
+// kernel).
 __device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int G, int qn, int tn, int X, int O,
                               int E, uint32_t* runs, const uint32_t* auxs, const AffDir* dir_top, bool done,
                               bool failed, int s_end, int t_end, int k_end, int layer_end, int row_g = 0,
-                              int row_w = 0, int row_lo = 0, const uint32_t* sh_hist = nullptr, int sh_rows = 0) {
+                              int row_w = 0, int row_lo = 0, const uint32_t* sh_hist = nullptr, int sh_rows = 0,
+                              bool folded = false) {
     const int gl = lane_id() & (G - 1);
     auto dir_at = [&](int64_t sc) -> const AffDir& { return dir_top[-1 - sc]; };
     auto aux_at = [&](int ss, int layer, int k) -> uint32_t {
+        if (folded) {
+            // one word per diagonal of the score's M band (the CTA kernel's layout)
+            const LayerBand& b = dir_at(ss).L[0];
+            const uint32_t w = auxs[b.base + (k - b.lo)];
+            return layer == 0 ? (((w >> 4) << 2) | (w & 3u)) : (w >> (layer + 1)) & 1u;
+        }
         if (row_g > 0) {
             // rows below sh_rows of diagonals -16..15 live in shared memory
             const int rr = ss / row_g;
@@ -1153,11 +1187,17 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
 // ===========================================================================
 // The warp-group kernel above runs a long, divergent pair with 32 lanes over bands of
 // thousands of diagonals per score, and only a few hundred such pairs exist in a batch:
-// most SMs idle. Here a CTA of kBigThreads threads takes one pair; the recurrence, cell
-// layout, band directory, candidate order and tie-breaks are those of wfa_affine_group
-// (values, ops and the end cell are identical), the diagonals of each score are dealt to
-// the CTA's threads, both sequences sit in shared memory (bulk copies), and one warp
-// walks the traceback.
+// most SMs idle. Here a CTA of kBigThreads threads takes one pair; the recurrence, band
+// rules, candidate order and tie-breaks are those of wfa_affine_group (values, ops and
+// the end cell are identical), the diagonals of each score are dealt to the CTA's
+// threads, both sequences sit in shared memory (bulk copies) while they fit, and one
+// warp walks the traceback.
+// Memory: the recurrence reads values at most max(X, O + E) scores back, so the M, I and
+// D values live in a ring of that many score slots, indexed by diagonal; what every
+// score keeps is one 32-bit history word per diagonal of its M band (the M source and
+// the M value before extension, plus the I and D extend bits; the bands of I and D lie
+// inside M's) and a directory entry with the three bands: 4 bytes per cell instead of
+// 8 per cell and layer.
 template <class S>
 __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
                                uint64_t region_bytes, uint32_t* sm, uint64_t* bar, uint32_t& phase, int* sh_red) {
@@ -1169,17 +1209,37 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
     uint32_t *qb, *tb;
     stage_pair_cta<S>(P, d, sm, bar, phase, &qb, &tb);
 
-    // region layout of wfa_affine_group: [runs][values][aux][... directory growing down]
+    int g = 0;
+    for (int v : {X, O, E}) {
+        int a = g, b = v < 0 ? -v : v;
+        while (b) {
+            const int t = a % b;
+            a = b;
+            b = t;
+        }
+        g = a;
+    }
+    const int step = g > 0 ? g : 1;
+    // value ring: slot (score / step) % ring_n, layers M, I, D, indexed by k + tn
+    const int ring_n = max(max(X, O + E), 1) / step + 1;
+    const uint64_t ring_w = static_cast<uint64_t>(qn + tn + 1);
+
+    // region: [runs][value ring][history words ...][... directory growing down]
     uint32_t* runs = reinterpret_cast<uint32_t*>(region);
     const uint64_t runs_bytes = align16(static_cast<uint64_t>(qn + tn + 2) * 4);
-    const uint64_t rest = region_bytes > runs_bytes ? region_bytes - runs_bytes : 0;
-    const uint64_t dir_cap = (rest / 4) / sizeof(AffDir);
+    const uint64_t ring_bytes = align16(static_cast<uint64_t>(ring_n) * 3 * ring_w * 4);
+    const uint64_t fixed = runs_bytes + ring_bytes;
+    const uint64_t rest = region_bytes > fixed ? region_bytes - fixed : 0;
+    const uint64_t dir_cap = (rest / 8) / sizeof(AffDir);
     const uint64_t cell_bytes = rest - rest % sizeof(AffDir) - dir_cap * sizeof(AffDir);
-    const uint64_t cell_cap = min(static_cast<uint64_t>((cell_bytes / 8) & ~3ull), static_cast<uint64_t>(0xFFFFFFFFu));
-    int32_t* vals = reinterpret_cast<int32_t*>(region + runs_bytes);
-    uint32_t* auxs = reinterpret_cast<uint32_t*>(vals + cell_cap);
-    AffDir* dir_top = reinterpret_cast<AffDir*>(region + runs_bytes + rest - (rest % sizeof(AffDir)));
+    const uint64_t cell_cap = min(static_cast<uint64_t>((cell_bytes / 4) & ~3ull), static_cast<uint64_t>(0xFFFFFFFFu));
+    int32_t* ring = reinterpret_cast<int32_t*>(region + runs_bytes);
+    uint32_t* auxs = reinterpret_cast<uint32_t*>(region + fixed);
+    AffDir* dir_top = reinterpret_cast<AffDir*>(region + fixed + rest - (rest % sizeof(AffDir)));
     auto dir_at = [&](int64_t sc) -> AffDir& { return dir_top[-1 - sc]; };
+    auto val = [&](int64_t sc, int layer, int k) -> int32_t* {
+        return ring + (static_cast<uint64_t>((sc / step) % ring_n) * 3 + layer) * ring_w + (k + tn);
+    };
     auto fits = [&](uint64_t ncells, int64_t nscores) -> bool {
         return ncells <= cell_cap && static_cast<uint64_t>(nscores) <= dir_cap;
     };
@@ -1192,21 +1252,23 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
     int s_end = 0, t_end = 0, k_end = 0, layer_end = 0;
     uint32_t used = 0;
     uint32_t wf_cells = 0, lcp_words = 0;
-    if (dir_cap < 1 || cell_cap < 1 || !fits(1, 1)) overflow = true;
+    int32_t reach = 0;  // furthest query offset this thread's cells reached (redo sizing)
+    if (region_bytes <= fixed || dir_cap < 1 || cell_cap < 1 || !fits(1, 1)) overflow = true;
     // ---- s = 0 ----
     if (!overflow && tid == 0) {
         AffDir e;
         e.L[0] = LayerBand{0, 0, 0};
-        e.L[1] = LayerBand{1, 0, 1};
-        e.L[2] = LayerBand{1, 0, 1};
+        e.L[1] = LayerBand{1, 0, 0};
+        e.L[2] = LayerBand{1, 0, 0};
         dir_at(0) = e;
-        vals[0] = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
+        *val(0, 0, 0) = extend_valid<S>(qb, qn, tb, tn, 0, 0, lcp_words);
         auxs[0] = 0;
     }
     __syncthreads();
     if (!overflow) {
         used = 1;
-        const int v0 = vals[0];
+        const int v0 = *val(0, 0, 0);
+        reach = v0;
         if (!fitting) {
             if (qn - tn == 0 && v0 == qn) {
                 done = true;
@@ -1218,17 +1280,6 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
         }
     }
     const SBand none = {1, 0, 0u};
-    int g = 0;
-    for (int v : {X, O, E}) {
-        int a = g, b = v < 0 ? -v : v;
-        while (b) {
-            const int t = a % b;
-            a = b;
-            b = t;
-        }
-        g = a;
-    }
-    const int step = g > 0 ? g : 1;
     int64_t s = step;
     // every thread computes the same bands and counters from the directory, so control
     // flow is uniform across the CTA
@@ -1261,63 +1312,63 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
         bM.lo = max(lo, -tn);
         bM.hi = min(hi, qn);
         if (tid == 0 && bM.lo <= bM.hi) wf_cells += static_cast<uint32_t>(bM.hi - bM.lo + 1);
-        const uint32_t wI = bI.lo <= bI.hi ? static_cast<uint32_t>(bI.hi - bI.lo + 1) : 0;
-        const uint32_t wD = bD.lo <= bD.hi ? static_cast<uint32_t>(bD.hi - bD.lo + 1) : 0;
         const uint32_t wM = bM.lo <= bM.hi ? static_cast<uint32_t>(bM.hi - bM.lo + 1) : 0;
-        bI.base = used;
-        bD.base = used + wI;
-        bM.base = used + wI + wD;
-        if (!fits(static_cast<uint64_t>(used) + wI + wD + wM, s + 1)) {
+        bM.base = used;
+        bI.base = bD.base = used;  // their history bits sit in M's words
+        if (!fits(static_cast<uint64_t>(used) + wM, s + 1)) {
             overflow = true;
             break;
         }
-        used += wI + wD + wM;
+        used += wM;
         int best_end_k = INT32_MAX, best_end_layer = 0;
-        for (int k = bM.lo + tid; k <= bM.hi; k += nthr) {
+        // (an empty band has lo = INT32_MAX, where lo + tid would wrap: its k loop starts
+        // past hi)
+        const int k0 = wM > 0 ? bM.lo + tid : 1, k1 = wM > 0 ? bM.hi : 0;
+        for (int k = k0; k <= k1; k += nthr) {
             int32_t ins = UNSET, del = UNSET;
+            uint32_t iop = 0, dop = 0;
             if (k >= bI.lo && k <= bI.hi) {
-                int32_t best = UNSET, iop = 0;
+                int32_t best = UNSET;
                 if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
-                    const int32_t c = vals[sMo.base + (k - 1 - sMo.lo)] + 1;
+                    const int32_t c = *val(so, 0, k - 1) + 1;
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 0; }
                 }
                 if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
-                    const int32_t c = vals[sIe.base + (k - 1 - sIe.lo)] + 1;
+                    const int32_t c = *val(se, 1, k - 1) + 1;
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 1; }
                 }
                 ins = best;
-                vals[bI.base + (k - bI.lo)] = ins;
-                auxs[bI.base + (k - bI.lo)] = static_cast<uint32_t>(iop);
+                *val(s, 1, k) = ins;
             }
             if (k >= bD.lo && k <= bD.hi) {
-                int32_t best = UNSET, dop = 0;
+                int32_t best = UNSET;
                 if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
-                    const int32_t c = vals[sMo.base + (k + 1 - sMo.lo)];
+                    const int32_t c = *val(so, 0, k + 1);
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 0; }
                 }
                 if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
-                    const int32_t c = vals[sDe.base + (k + 1 - sDe.lo)];
+                    const int32_t c = *val(se, 2, k + 1);
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 1; }
                 }
                 del = best;
-                vals[bD.base + (k - bD.lo)] = del;
-                auxs[bD.base + (k - bD.lo)] = static_cast<uint32_t>(dop);
+                *val(s, 2, k) = del;
             }
             int32_t best = UNSET;
             uint32_t mop = 0;
             if (k >= sMx.lo && k <= sMx.hi) {
-                const int32_t c = vals[sMx.base + (k - sMx.lo)] + 1;
+                const int32_t c = *val(sx, 0, k) + 1;
                 if (pos_ok(c, k, qn, tn)) { best = c; mop = 0; }
             }
             if (pos_ok(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
             if (pos_ok(del, k, qn, tn) && del > best) { best = del; mop = 2; }
             int32_t mval = UNSET;
-            uint32_t aux = 0;
+            uint32_t aux = (dop << 3) | (iop << 2);
             if (best != UNSET) {
                 mval = extend_valid<S>(qb, qn, tb, tn, best, k, lcp_words);
-                aux = (static_cast<uint32_t>(best) << 2) | mop;
+                aux |= (static_cast<uint32_t>(best) << 4) | mop;
+                reach = max(reach, mval);
             }
-            vals[bM.base + (k - bM.lo)] = mval;
+            *val(s, 0, k) = mval;
             auxs[bM.base + (k - bM.lo)] = aux;
             const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
             if (layer >= 0) {
@@ -1347,7 +1398,7 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
         __syncthreads();  // this score's cells, directory entry and partial minima are visible
         long long best = LLONG_MAX;
         for (int w = 0; w < nthr / 32; ++w) best = min(best, red[w]);
-        __syncthreads();  // `red` is rewritten by the next score
+        __syncthreads();  // `red` and the ring slot of s - ring_n * step are rewritten next
         if (best != LLONG_MAX) {
             done = true;
             s_end = static_cast<int>(s);
@@ -1362,17 +1413,41 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
         if (lcp_words) atomicAdd(P.work + 3, static_cast<unsigned long long>(lcp_words));
     }
     const bool failed = !done && !overflow;
-    if (overflow && tid == 0) {
-        const uint64_t full = runs_bytes + 4ull * static_cast<uint64_t>(hard_max_s + 1) * sizeof(AffDir) +
-                              static_cast<uint64_t>(hard_max_s + 1) * 3ull * static_cast<uint64_t>(qn + tn + 1) * 8ull + 4096;
-        const uint64_t grow = runs_bytes + 4ull * (static_cast<uint64_t>(used) * 8 + static_cast<uint64_t>(s + 1) * sizeof(AffDir)) +
-                              4096;
-        report_redo(P, pid, min(full, grow));
+    if (overflow) {  // CTA-uniform
+        // Scratch for the redo: extrapolate the final score from the furthest query offset
+        // reached so far (the wavefront advances about in proportion to the score), plus a
+        // quarter as margin, and the history from the cells so far (bands grow linearly,
+        // so cells grow with the square of the score); at least four times what was used,
+        // at most the whole search.
+        long long* red = reinterpret_cast<long long*>(sh_red);
+        int32_t wr = reach;
+        for (int o = 16; o > 0; o >>= 1) wr = max(wr, __shfl_xor_sync(PHR_FULL_MASK, wr, o));
+        if ((tid & 31) == 0) red[tid >> 5] = wr;
+        __syncthreads();
+        if (tid == 0) {
+            int64_t rmax = 0;
+            for (int w = 0; w < nthr / 32; ++w) rmax = ::max(rmax, static_cast<int64_t>(red[w]));
+            const uint64_t full_cells = static_cast<uint64_t>(hard_max_s / step + 1) * ring_w;
+            uint64_t s_est = static_cast<uint64_t>(hard_max_s) + 1, cells = full_cells;
+            if (rmax > 0 && s > step) {
+                uint64_t e = static_cast<uint64_t>(s) * static_cast<uint64_t>(qn) / static_cast<uint64_t>(rmax);
+                e += e / 4 + 64;
+                if (e < s_est) {
+                    s_est = e;
+                    const double r = static_cast<double>(e) / static_cast<double>(s);
+                    cells = ::min(full_cells, static_cast<uint64_t>(static_cast<double>(used) * r * r) + 1024);
+                }
+            }
+            cells = ::max(cells, static_cast<uint64_t>(4ull * used + 1024));
+            const uint64_t need_rest =
+                ::max(static_cast<uint64_t>(cells * 4 * 8 / 7 + 4096), static_cast<uint64_t>(8 * (s_est + 1) * sizeof(AffDir))) + 64;
+            report_redo(P, pid, fixed + need_rest + 4096);
+        }
     }
     __syncthreads();
     if (tid < 32)
         affine_finish(P, pid, true, 32, qn, tn, X, O, E, runs, auxs, dir_top, done, failed, s_end, t_end, k_end,
-                      layer_end);
+                      layer_end, 0, 0, 0, nullptr, 0, true);
     __syncthreads();
 }
 
@@ -1445,9 +1520,30 @@ __device__ __forceinline__ int32_t reg_neighbor(const int32_t (&v)[kRegSlots], i
 // scores 0 .. (kRegShRows - 1) g, which hold the whole history of most short pairs, so
 // their traceback reads shared memory.
 constexpr int kRegShRows = 32;
+// Words of a short pair's two staged sequences (qlen + tlen < kRegMaxLen, each followed by
+// one padding word for the 32-bit windows that read one word ahead).
+constexpr int kRegSeqWords = 1024 / 16 + 4;
+// Shared memory of one warp on the register path: the history rows, then the staged
+// sequences of its pair.
+constexpr int kRegWarpSmem = kRegShRows * 128 + kRegSeqWords * 4;
 
+// Copies a short 2-bit pair's words into `dst` (q first, then t) with the W lanes of
+// its segment; the caller synchronises the warp before reading them. Match extension
+// then reads shared memory instead of L1/L2.
+template <int W>
+__device__ __forceinline__ void stage_pair_words(uint32_t* dst, const uint32_t* q, int qn, const uint32_t* t, int tn,
+                                                 int ls, const uint32_t** sq, const uint32_t** st) {
+    const int qw = (qn + 15) / 16 + 1, tw = (tn + 15) / 16 + 1;
+    for (int i = ls; i < qw; i += W) dst[i] = __ldg(q + i);
+    for (int i = ls; i < tw; i += W) dst[qw + i] = __ldg(t + i);
+    *sq = dst;
+    *st = dst + qw;
+}
+
+// Returns true when the pair's band left the window: nothing is written for it and the
+// caller runs it through wfa_affine_group.
 template <class S, int XS, int OES, int ES>
-__device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
+__device__ bool wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_t pid, uint8_t* region,
                                uint64_t region_bytes, uint32_t* sh_hist) {
     constexpr int RM = (XS > OES ? XS : OES);  // M values kept: steps 1..RM back
     const int lane = lane_id();
@@ -1455,8 +1551,10 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
     const bool fitting = tn > qn + qn / 2 + 10;
     const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
     const int g = X / XS;  // the step of reachable scores
-    const uint32_t* qb = seq_base<S>(P, d.q_word);
-    const uint32_t* tb = seq_base<S>(P, d.t_word);
+    const uint32_t *qb, *tb;
+    stage_pair_words<32>(sh_hist + kRegShRows * 32, seq_base<S>(P, d.q_word), qn, seq_base<S>(P, d.t_word), tn, lane,
+                         &qb, &tb);
+    __syncwarp();
     const int64_t hard_max_s = static_cast<int64_t>(qn + tn) * max(X, 1) + O + E + 4;
 
     // region: [runs][aux rows: kRegWin words per visited score, each word the M, I and D
@@ -1639,19 +1737,16 @@ __device__ void wfa_affine_reg(const ExtendParams& P, const PairDesc& d, uint32_
             atomicAdd(P.work + 3, static_cast<unsigned long long>(lw));
         }
     }
-    if (overflow) {
-        // redo with wfa_affine_group, which sizes its bands per score
-        if (lane == 0) report_redo(P, pid, wfa_region_est(qn, tn, true));
-        return;
-    }
     __syncwarp();
+    if (overflow) return true;  // wfa_affine_group takes it, which sizes its bands per score
     affine_finish(P, pid, true, 32, qn, tn, X, O, E, runs, auxs, nullptr, done, !done, s_end, t_end, k_end,
                   layer_end, g, kRegWin, kRegLo, sh_hist, kRegShRows);
+    return false;
 }
 
 // Persistent kernel: warps pull tasks; each task's groups split the warp's slot evenly.
 constexpr int kAffGroupSmem = kAffRingGroups * kAffRing * static_cast<int>(sizeof(SDir)) + kWarpSeqWords * 4;
-constexpr int kAffWarpSmem = kAffGroupSmem > kRegShRows * 128 ? kAffGroupSmem : kRegShRows * 128;
+constexpr int kAffWarpSmem = kAffGroupSmem > kRegWarpSmem ? kAffGroupSmem : kRegWarpSmem;
 
 template <class S, bool kAffine>
 __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams P) {
@@ -1698,14 +1793,12 @@ __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams 
                 const int X = P.costs.mismatch, O = P.costs.gap_open, E = P.costs.gap_extend;
                 uint32_t* sh_hist = reinterpret_cast<uint32_t*>(wfa_smem + static_cast<size_t>(threadIdx.x >> 5) *
                                                                                   kAffWarpSmem);
-                if (X == 4 && O == 6 && E == 2) {
-                    wfa_affine_reg<S, 2, 4, 1>(P, d, pid, region, region_bytes, sh_hist);
-                    continue;
-                }
-                if (X == 2 && O == 4 && E == 1) {
-                    wfa_affine_reg<S, 2, 5, 1>(P, d, pid, region, region_bytes, sh_hist);
-                    continue;
-                }
+                bool wide = true;  // the band left the register window (or no specialisation)
+                if (X == 4 && O == 6 && E == 2) wide = wfa_affine_reg<S, 2, 4, 1>(P, d, pid, region, region_bytes, sh_hist);
+                else if (X == 2 && O == 4 && E == 1)
+                    wide = wfa_affine_reg<S, 2, 5, 1>(P, d, pid, region, region_bytes, sh_hist);
+                if (!wide) continue;
+                // otherwise the group kernel below takes the pair in place (no redo pass)
             }
         }
         if (kAffine) {
