@@ -977,6 +977,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             uint64_t tot = 0;
             while (pos < idx.size()) {
                 uint64_t need = (std::max<uint64_t>(h_rneed[idx[pos]], 4096) + 255) & ~255ull;
+                bool clamp = false;
                 if (need > ctx->scratch_budget) {
                     // first-pass needs are estimates: try once with the whole budget
                     if (clamped.count(h_list[idx[pos]])) {
@@ -986,10 +987,12 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                         ++pos;
                         continue;
                     }
-                    clamped.insert(h_list[idx[pos]]);
+                    clamp = true;
                     need = ctx->scratch_budget & ~255ull;
                 }
-                if (!pl.empty() && tot + need > ctx->scratch_budget) break;
+                if (!pl.empty() && tot + need > ctx->scratch_budget) break;  // this pair opens the next pass
+                // the whole-budget try is spent only once the pair is placed in a pass
+                if (clamp) clamped.insert(h_list[idx[pos]]);
                 pl.push_back(h_list[idx[pos]]);
                 po.push_back(tot);
                 pn.push_back(need);

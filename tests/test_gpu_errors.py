@@ -41,6 +41,24 @@ def test_workspace_too_small_is_per_pair_oom():
         assert P.unpack(ga, gc) == P.unpack(oa, oc)
 
 
+def test_estimates_above_budget_each_get_the_whole_budget():
+    """Several long pairs whose first scratch estimate exceeds the budget each get one try
+    with the whole budget, in a pass of its own; a pair that fits then is aligned, not
+    reported out of memory because an earlier pair took the pass."""
+    rng = np.random.default_rng(33)
+    pairs = []
+    for _ in range(3):
+        q = bytearray(rng.choice(list(b"ACGT"), 24000).tolist())
+        t = bytearray(q)
+        for p in rng.choice(len(t), 120, replace=False):
+            t[p] = b"ACGT"[(b"ACGT".index(t[p]) + 1) % 4]
+        pairs.append((bytes(q), bytes(t)))
+    with P.Engine(0, workspace_bytes=1 << 20) as eng:
+        got = eng.extend(A.ENGINE_WFA_LINEAR, pairs)
+        assert eng.counter("scratch_oom_pairs") == 0
+    assert got == O.extend(A.ENGINE_WFA_LINEAR, pairs)
+
+
 def test_bad_arguments_are_refused():
     with P.Engine(0) as eng:
         L = eng._lib
