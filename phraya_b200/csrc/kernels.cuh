@@ -88,38 +88,6 @@ __host__ __device__ __forceinline__ uint64_t wfa_region_est(int qn, int tn, bool
     return 16 * L + 4 * cells + 4096;
 }
 
-// First scratch estimate of a gap-affine pair run one per CTA (wfa_affine_cta), in that
-// kernel's layout: the run list, a ring of max(X, O + E) / g + 1 value slots of three
-// layers, then one 4-byte history word per cell of each visited score's M band (7/8 of
-// the rest) and a 48-byte directory entry per score (1/8). Scores are taken up to
-// 64 + qn (X + O + E) / 24, about what a read with 5 % errors (substitutions and short
-// indels) costs; the M band at score s spans 2 (s - O) / E + 1 diagonals, visited every
-// g = gcd(X, O, E). Pairs that need more overflow once and are redone with what they ask.
-__host__ __device__ __forceinline__ uint64_t wfa_affine_big_est(int qn, int tn, int X, int O, int E) {
-    int g = 0;
-    for (int v : {X, O, E}) {
-        int a = g, b = v < 0 ? -v : v;
-        while (b) {
-            const int t = a % b;
-            a = b;
-            b = t;
-        }
-        g = a;
-    }
-    const uint64_t step = g > 0 ? static_cast<uint64_t>(g) : 1;
-    const uint64_t e = E > 0 ? static_cast<uint64_t>(E) : 1;
-    const uint64_t L = static_cast<uint64_t>(qn + tn);
-    const uint64_t ring_n = static_cast<uint64_t>(X > O + E ? X : O + E) / step + 1;
-    const uint64_t fixed = ((L + 2) * 4 + 15) / 16 * 16 + (ring_n * 3 * (L + 1) * 4 + 15) / 16 * 16;
-    const uint64_t s = 64 + static_cast<uint64_t>(qn) * static_cast<uint64_t>(X + O + E) / 24;
-    uint64_t width = 2 * s / e + 1;
-    if (width > L + 1) width = L + 1;
-    const uint64_t cells = (s / step + 1) * ((width + 1) / 2 + 1);  // the bands grow linearly
-    const uint64_t rest_cells = cells * 4 * 8 / 7 + 4096;
-    const uint64_t rest_dir = 8 * (s + 1) * 48;
-    return fixed + (rest_cells > rest_dir ? rest_cells : rest_dir) + 8192;
-}
-
 // ---------------------------------------------------------------------------
 // Lane-per-pair banded Myers (global mode, 2-bit pairs; myers_lane.cu).
 //

@@ -1775,9 +1775,7 @@ __global__ void __launch_bounds__(256, kAffine ? 2 : 4) wfa_kernel(ExtendParams 
         // where wfa_linear_big_kernel / wfa_affine_big_kernel take them
         if (act && !P.task_off && big_pair(P.engine, P.big_min, P.big_smem, d.qn, d.tn, d.mode)) {
             if ((lane & (G - 1)) == 0)
-                report_redo(P, pid,
-                            kAffine ? wfa_affine_big_est(d.qn, d.tn, P.costs.mismatch, P.costs.gap_open, P.costs.gap_extend)
-                                    : wfa_region_est(d.qn, d.tn, false));
+                report_redo(P, pid, wfa_region_est(d.qn, d.tn, kAffine));
             act = false;
         }
         if (!__any_sync(PHR_FULL_MASK, act)) continue;
