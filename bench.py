@@ -113,7 +113,7 @@ def packed_bytes(p):
     return 4.0 * float(((p.q_len.astype(np.int64) + 15) // 16).sum() + ((p.t_len.astype(np.int64) + 15) // 16).sum())
 
 
-SEG_COLS = 4  # columns per recomputed traceback segment of the checkpointed lane kernel
+SEG_COLS = 8  # columns per recomputed traceback segment of the checkpointed lane kernel
 
 
 def traffic_record(kernel):
@@ -127,10 +127,14 @@ def traffic_record(kernel):
         rec = json.load(f).get(kernel)
     if not rec:
         return None, "no capture record for this kernel"
-    with open(os.path.join(ROOT, rec["source"]), "rb") as f:
-        sha = hashlib.sha256(f.read()).hexdigest()
-    if sha != rec["source_sha256"]:
-        return None, f"capture record is of another version of {rec['source']}"
+    # the record names the kernel's source files; their concatenation's SHA-256 must match
+    srcs = rec["sources"] if "sources" in rec else [rec["source"]]
+    h = hashlib.sha256()
+    for src in srcs:
+        with open(os.path.join(ROOT, src), "rb") as f:
+            h.update(f.read())
+    if h.hexdigest() != rec["source_sha256"]:
+        return None, f"capture record is of another version of {' + '.join(srcs)}"
     return rec["dram_bytes"] / rec["pairs"], (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
                                               f"{rec['pairs']} pairs ({rec['dram_bytes'] / 1e9:.2f} GB), per pair "
                                               f"x pairs; command: {rec['command']}")

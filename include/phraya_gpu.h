@@ -142,7 +142,7 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *   "host_chunks"                        chunks a host batch of more than 128 MiB of sequence
  *                                        is copied and aligned in, overlapped (2..32, default 4)
  *   "myers_lane_ckpt"                    banded Myers (global 2-bit pairs): 1 = keep the band's
- *                                        state every 4th column and recompute 4 columns at a
+ *                                        state every 8th column and recompute 8 columns at a
  *                                        time for the traceback (default), 0 = store every
  *                                        column's records
  * With phr_config.tune_file_enable, phr_ctx_create applies "key value" lines of the tune

@@ -903,7 +903,10 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
         if (per_task && (engine == PHR_ENGINE_WFA_LINEAR || engine == PHR_ENGINE_WFA_AFFINE) && P.big_min > 0 &&
             n_tasks_hint > 0) {
             // long pairs of this redo list, one CTA each
-            const uint64_t big_per_sm = ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1;
+            // linear: two CTAs of kBigThreads per SM (one when the tune keeps fewer blocks
+            // resident); gap-affine: one CTA of kBigAffineThreads
+            const uint64_t big_per_sm =
+                engine == PHR_ENGINE_WFA_AFFINE ? 1 : (ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1);
             const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, ctx->sm_count * big_per_sm));
             PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 24, 0, 8, st));
             for (int mode = 0; mode < 2; ++mode) {

@@ -33,7 +33,7 @@ struct DeviceArena {
 
 // Tunables of one engine; filled from the autotuner cache when present.
 struct EngineTune {
-    int wfa_group_short = 4;     // lanes per pair for linear WFA pairs with qn+tn < wfa_long_min
+    int wfa_group_short = 8;     // lanes per pair for linear WFA pairs with qn+tn < wfa_long_min
     int wfa_affine_group_short = 32;  // the same for gap-affine WFA pairs (32: one pair per warp, wavefronts in registers)
     int wfa_group_long = 32;
     int wfa_long_min = 1024;     // bucket edge: qn+tn from which WFA pairs get wfa_group_long lanes

@@ -49,7 +49,12 @@ struct ExtendParams {
 
 // task_group bit marking a redo task for the CTA-per-pair kernel
 constexpr uint8_t kBigTask = 0x80;
-constexpr int kBigThreads = 512;
+constexpr int kBigThreads = 512;         // threads of the linear CTA-per-pair kernel (two CTAs per SM)
+// threads of the gap-affine CTA-per-pair kernel (one CTA per SM): its cells cost three
+// layers, so a score's band takes longer than its barrier and more threads per pair pay
+// (1024: 1.33 s against 2.00 s with 512 for 20 sensitive long reads; linear, whose band
+// is cheap per cell, measured 87 against 78 ms with 1024)
+constexpr int kBigAffineThreads = 1024;
 constexpr uint32_t kBigMinFrameCells = 4096;  // smallest shared frame pair worth staging
 
 // Shared-memory words the CTA-per-pair kernel needs for the two sequences of a pair:
@@ -129,8 +134,10 @@ __host__ __device__ __forceinline__ int lane_slots(int dmin, int dmax, int nb) {
 
 // Columns per traceback segment of the checkpointed lane kernel: the forward pass keeps
 // the window's {VP, VN} after every kSegCols-th column, the traceback recomputes one
-// segment of columns at a time into shared memory.
-constexpr int kSegCols = 4;
+// segment of columns at a time into the task's scratch slot and walks it. Per 1,000,000
+// pairs of 64-2048 bp: 8 columns 13.43 ms, 4 columns 13.76 ms, 2 columns 15.90 ms (the
+// recompute is the same work; fewer checkpoints are fewer stores and dependent loads).
+constexpr int kSegCols = 8;
 
 // Scratch of one lane task, then one reverse-run list of (m_max + n_max + 2) words per
 // lane. Record mode: 16-byte {VP, HP} records [column group][slot][lane][column in

@@ -1187,7 +1187,7 @@ __device__ void wfa_affine_group(const ExtendParams& P, const PairDesc& d, uint3
 // ===========================================================================
 // The warp-group kernel above runs a long, divergent pair with 32 lanes over bands of
 // thousands of diagonals per score, and only a few hundred such pairs exist in a batch:
-// most SMs idle. Here a CTA of kBigThreads threads takes one pair; the recurrence, band
+// most SMs idle. Here a CTA of kBigAffineThreads threads takes one pair; the recurrence, band
 // rules, candidate order and tie-breaks are those of wfa_affine_group (values, ops and
 // the end cell are identical), the diagonals of each score are dealt to the CTA's
 // threads, both sequences sit in shared memory (bulk copies) while they fit, and one
@@ -1452,10 +1452,10 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
 }
 
 template <class S>
-__global__ void __launch_bounds__(kBigThreads, 2) wfa_affine_big_kernel(ExtendParams P) {
+__global__ void __launch_bounds__(kBigAffineThreads, 1) wfa_affine_big_kernel(ExtendParams P) {
     extern __shared__ __align__(16) uint32_t big_sm[];
     __shared__ uint32_t sh_task;
-    __shared__ __align__(8) long long sh_red[kBigThreads / 32];
+    __shared__ __align__(8) long long sh_red[kBigAffineThreads / 32];
     __shared__ __align__(8) uint64_t sh_bar;
     uint32_t phase = 0;  // parity of sh_bar's current phase, the same in every thread
     if (threadIdx.x == 0) mbar_init(&sh_bar, 1);
@@ -1840,11 +1840,11 @@ void launch_wfa_affine_big(const ExtendParams& p, int grid, int mode, cudaStream
     if (mode == 0) {
         cudaFuncSetAttribute(wfa_affine_big_kernel<Seq2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(p.big_smem));
-        wfa_affine_big_kernel<Seq2><<<grid, kBigThreads, p.big_smem, st>>>(p);
+        wfa_affine_big_kernel<Seq2><<<grid, kBigAffineThreads, p.big_smem, st>>>(p);
     } else {
         cudaFuncSetAttribute(wfa_affine_big_kernel<SeqB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(p.big_smem));
-        wfa_affine_big_kernel<SeqB><<<grid, kBigThreads, p.big_smem, st>>>(p);
+        wfa_affine_big_kernel<SeqB><<<grid, kBigAffineThreads, p.big_smem, st>>>(p);
     }
 }
 
