@@ -114,6 +114,7 @@ def packed_bytes(p):
 
 
 SEG_COLS = 8  # columns per recomputed traceback segment of the checkpointed lane kernel
+REF_SAMPLE_A = 20000  # set-A pairs per step of the reference arm (set B in the job's proportion)
 
 
 def traffic_record(kernel):
@@ -247,9 +248,11 @@ def prefix(p, k):
 def run_reference(args, rank, world):
     """Reference arm: the reference's CPU algorithm on the host cores, all threads. The
     Rust reference cannot be built without a Rust toolchain, so this is the oracle
-    restatement (kind "port"). Each step aligns the first 60,000 set-A pairs (WFA affine
-    4/6/2 and WFA linear) and the first 6,000 set-B pairs (Myers) of exactly the pairs the
-    engine arm aligns; the step's time is that sample's measured time."""
+    restatement (kind "port"). Each step aligns the first REF_SAMPLE_A set-A pairs (WFA
+    affine 4/6/2 and WFA linear) and as many set-B pairs (Myers) as keep the engine arm's
+    mix of the three alignment sets, of exactly the pairs the engine arm aligns; the
+    step's time is that sample's measured time, so `value` is the job's rate on its own
+    mix."""
     if rank != 0:
         return
     import oracle as O
@@ -258,7 +261,9 @@ def run_reference(args, rank, world):
 
     nthreads = os.cpu_count() or 1
     da, db = arm_pairs(args.n_a, args.n_b, 0, 0)
-    set_a, set_b = prefix(D.to_packed(da), 60000), prefix(D.to_packed(db), 6000)
+    na = min(args.n_a, REF_SAMPLE_A)
+    nb = min(args.n_b, max(1, round(na * args.n_b / max(args.n_a, 1))))
+    set_a, set_b = prefix(D.to_packed(da), na), prefix(D.to_packed(db), nb)
     del da, db
     L = O.lib()
     jobs = ((A.ENGINE_WFA_AFFINE, set_a, COSTS_A), (A.ENGINE_WFA_LINEAR, set_a, (2, 4, 1)),
@@ -279,8 +284,9 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded)",
             "config": {"workload": "batched extension microbench", "n_pairs_wfa": set_a.n, "n_pairs_myers": set_b.n,
-                       "pairs": "the first 60,000 set-A and 6,000 set-B pairs of the engine arm's 1,000,000 + "
-                                "1,000,000 (same generator, same seeds)",
+                       "pairs": f"the first {set_a.n} set-A and {set_b.n} set-B pairs of the engine arm's "
+                                f"{args.n_a} + {args.n_b} (same generator, same seeds, same mix of the three "
+                                "alignment sets)",
                        "note": "CPU restatement of phraya-align (Rust toolchain absent), all host threads"},
             "projected_full_job_ms": (2 * args.n_a + args.n_b) / v * 1000.0,
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": nthreads, "kind": "port",
