@@ -808,7 +808,8 @@ __device__ void affine_finish(const ExtendParams& P, uint32_t pid, bool act, int
         }
         if (row_g > 0) {
             // rows below sh_rows of diagonals -16..15 live in shared memory
-            const int rr = ss / row_g;
+            // row of score ss (a multiple of g; g is 1 or 2 for the specialised costs)
+            const int rr = row_g == 1 ? ss : row_g == 2 ? (ss >> 1) : ss / row_g;
             const uint32_t w = (rr < sh_rows && static_cast<unsigned>(k + 16) < 32u)
                                    ? sh_hist[rr * 32 + (k + 16)]
                                    : auxs[static_cast<uint64_t>(rr) * row_w + (k - row_lo)];
@@ -1324,39 +1325,52 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
         // (an empty band has lo = INT32_MAX, where lo + tid would wrap: its k loop starts
         // past hi)
         const int k0 = wM > 0 ? bM.lo + tid : 1, k1 = wM > 0 ? bM.hi : 0;
+        // ring rows of this score's sources and of the score itself, indexed by diagonal
+        // (the slot arithmetic once per score, not per cell; a negative score's row is
+        // never read: its band is empty)
+        auto row = [&](int64_t sc, int layer) -> int32_t* {
+            return sc < 0 ? nullptr : val(sc, layer, 0);
+        };
+        const int32_t* rMo = row(so, 0);
+        const int32_t* rIe = row(se, 1);
+        const int32_t* rDe = row(se, 2);
+        const int32_t* rMx = row(sx, 0);
+        int32_t* cM = row(s, 0);
+        int32_t* cI = row(s, 1);
+        int32_t* cD = row(s, 2);
         for (int k = k0; k <= k1; k += nthr) {
             int32_t ins = UNSET, del = UNSET;
             uint32_t iop = 0, dop = 0;
             if (k >= bI.lo && k <= bI.hi) {
                 int32_t best = UNSET;
                 if (k - 1 >= sMo.lo && k - 1 <= sMo.hi) {
-                    const int32_t c = *val(so, 0, k - 1) + 1;
+                    const int32_t c = rMo[k - 1] + 1;
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 0; }
                 }
                 if (k - 1 >= sIe.lo && k - 1 <= sIe.hi) {
-                    const int32_t c = *val(se, 1, k - 1) + 1;
+                    const int32_t c = rIe[k - 1] + 1;
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; iop = 1; }
                 }
                 ins = best;
-                *val(s, 1, k) = ins;
+                cI[k] = ins;
             }
             if (k >= bD.lo && k <= bD.hi) {
                 int32_t best = UNSET;
                 if (k + 1 >= sMo.lo && k + 1 <= sMo.hi) {
-                    const int32_t c = *val(so, 0, k + 1);
+                    const int32_t c = rMo[k + 1];
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 0; }
                 }
                 if (k + 1 >= sDe.lo && k + 1 <= sDe.hi) {
-                    const int32_t c = *val(se, 2, k + 1);
+                    const int32_t c = rDe[k + 1];
                     if (pos_ok(c, k, qn, tn) && c > best) { best = c; dop = 1; }
                 }
                 del = best;
-                *val(s, 2, k) = del;
+                cD[k] = del;
             }
             int32_t best = UNSET;
             uint32_t mop = 0;
             if (k >= sMx.lo && k <= sMx.hi) {
-                const int32_t c = *val(sx, 0, k) + 1;
+                const int32_t c = rMx[k] + 1;
                 if (pos_ok(c, k, qn, tn)) { best = c; mop = 0; }
             }
             if (pos_ok(ins, k, qn, tn) && ins > best) { best = ins; mop = 1; }
@@ -1368,7 +1382,7 @@ __device__ void wfa_affine_cta(const ExtendParams& P, const PairDesc& d, uint32_
                 aux |= (static_cast<uint32_t>(best) << 4) | mop;
                 reach = max(reach, mval);
             }
-            *val(s, 0, k) = mval;
+            cM[k] = mval;
             auxs[bM.base + (k - bM.lo)] = aux;
             const int layer = mval == qn ? 0 : ins == qn ? 1 : del == qn ? 2 : -1;
             if (layer >= 0) {
