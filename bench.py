@@ -306,6 +306,9 @@ def run_one_case(args):
     int_peak = 148 * 4 * 32 * peaks.get("sm_max_mhz", 1965.0) * 1e6
     eng = P.Engine(dev, workspace_bytes=int(args.contig_workspace_gb * 2**30) if args.only_case == "contigs_protein"
                    else 0)
+    for kv in args.tune:  # launch-parameter overrides, as for the microbench
+        key, val = kv.split("=", 1)
+        eng.set_tune(key, int(val))
     if args.only_case == "case2_short":
         out = run_case2_short(eng, dev, args)
     elif args.only_case == "long_reads":
@@ -1052,7 +1055,8 @@ def main():
     ap.add_argument("--long-sensitive-parity", type=int, default=16,
                     help="long reads checked against the oracle (sensitive)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
-                    help="launch parameter of the microbench's engine (phr_ctx_set_tune), repeatable")
+                    help="launch parameter of the microbench's engine, or of the --only-case engine "
+                         "(phr_ctx_set_tune), repeatable")
     ap.add_argument("--contig-workspace-gb", type=float, default=4.0,
                     help="extension workspace of the contig case: a pair that needs more (an extension across an "
                          "inversion from a wrong anchor) reports a per-pair scratch failure, as a memory-bound host "

@@ -137,6 +137,8 @@ void phr_ctx_destroy(phr_ctx* ctx);
  *                                        >= this run one per CTA (0 = never)
  *   "wfa_big_smem"                       shared memory of those kernels, bytes (16 KiB..200
  *                                        KiB; longer pairs are read from global memory)
+ *   "wfa_affine_big_threads"             threads per CTA of the gap-affine one-CTA-per-pair
+ *                                        kernel: 1024 (default, one CTA per SM), 512 or 256
  *   "max_blocks_per_sm"                  resident blocks per SM of the persistent extension
  *                                        kernels (1..4)
  *   "host_chunks"                        chunks a host batch of more than 128 MiB of sequence

@@ -383,6 +383,7 @@ int* tune_field(phr::EngineTune& t, const char* key) {
     if (!std::strcmp(key, "wfa_long_min")) return &t.wfa_long_min;
     if (!std::strcmp(key, "host_chunks")) return &t.host_chunks;
     if (!std::strcmp(key, "myers_lane_ckpt")) return &t.myers_lane_ckpt;
+    if (!std::strcmp(key, "wfa_affine_big_threads")) return &t.wfa_affine_big_threads;
     return nullptr;
 }
 bool tune_valid(const char* key, int64_t v) {
@@ -397,6 +398,7 @@ bool tune_valid(const char* key, int64_t v) {
     if (!std::strcmp(key, "wfa_long_min")) return v >= 0 && v <= INT32_MAX;
     if (!std::strcmp(key, "host_chunks")) return v >= 2 && v <= 32;
     if (!std::strcmp(key, "myers_lane_ckpt")) return v == 0 || v == 1;
+    if (!std::strcmp(key, "wfa_affine_big_threads")) return v == 256 || v == 512 || v == 1024;
     return false;
 }
 }  // namespace

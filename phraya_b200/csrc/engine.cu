@@ -904,9 +904,11 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
             n_tasks_hint > 0) {
             // long pairs of this redo list, one CTA each
             // linear: two CTAs of kBigThreads per SM (one when the tune keeps fewer blocks
-            // resident); gap-affine: one CTA of kBigAffineThreads
-            const uint64_t big_per_sm =
-                engine == PHR_ENGINE_WFA_AFFINE ? 1 : (ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1);
+            // resident); gap-affine: kBigAffineThreads / wfa_affine_big_threads CTAs per SM
+            const int aff_threads = ctx->tune.wfa_affine_big_threads;
+            const uint64_t big_per_sm = engine == PHR_ENGINE_WFA_AFFINE
+                                            ? static_cast<uint64_t>(kBigAffineThreads / aff_threads)
+                                            : (ctx->tune.max_blocks_per_sm >= 4 ? 2 : 1);
             const int big_grid = static_cast<int>(std::min<uint64_t>(n_tasks_hint, ctx->sm_count * big_per_sm));
             PHR_CUDA_TRY(ctx, cudaMemsetAsync(cnt + 24, 0, 8, st));
             for (int mode = 0; mode < 2; ++mode) {
@@ -917,7 +919,7 @@ phr_status run_extend(Ctx* ctx, phr_engine engine, const DevPairs& in, phr_affin
                     launch_wfa_linear_big(P, big_grid, mode, st);
                 } else {
                     KernelScope ks(ctx, mode ? "wfa_affine_big_bytes" : "wfa_affine_big");
-                    launch_wfa_affine_big(P, big_grid, mode, st);
+                    launch_wfa_affine_big(P, big_grid, aff_threads, mode, st);
                 }
             }
         }

@@ -43,6 +43,8 @@ struct EngineTune {
     int wfa_big_smem = 100 << 10;    // shared memory of that kernel, bytes (two CTAs per SM)
     int max_blocks_per_sm = 4;       // resident blocks per SM of the persistent extension kernels
     int host_chunks = 4;             // chunks a large host batch is copied and aligned in (overlapped)
+    int wfa_affine_big_threads = kBigAffineThreads;  // threads per CTA of the gap-affine
+                                     // CTA-per-pair kernel (256, 512 or 1024; 1024 / this CTAs per SM)
     int myers_lane_ckpt = 1;         // banded Myers lane kernel: recompute segments from checkpoints (1)
                                      // or store every column's records (0)
 };

@@ -50,10 +50,8 @@ struct ExtendParams {
 // task_group bit marking a redo task for the CTA-per-pair kernel
 constexpr uint8_t kBigTask = 0x80;
 constexpr int kBigThreads = 512;         // threads of the linear CTA-per-pair kernel (two CTAs per SM)
-// threads of the gap-affine CTA-per-pair kernel (one CTA per SM): its cells cost three
-// layers, so a score's band takes longer than its barrier and more threads per pair pay
-// (1024: 1.33 s against 2.00 s with 512 for 20 sensitive long reads; linear, whose band
-// is cheap per cell, measured 87 against 78 ms with 1024)
+// most threads per CTA of the gap-affine CTA-per-pair kernel, and its default (one CTA
+// per SM; the "wfa_affine_big_threads" setting launches 512 or 256, two or four per SM)
 constexpr int kBigAffineThreads = 1024;
 constexpr uint32_t kBigMinFrameCells = 4096;  // smallest shared frame pair worth staging
 
@@ -179,6 +177,6 @@ constexpr int kLaneThreads = 256;
 void launch_wfa_linear(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_affine(const ExtendParams& p, int grid, int block, cudaStream_t st);
 void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
-void launch_wfa_affine_big(const ExtendParams& p, int grid, int mode, cudaStream_t st);
+void launch_wfa_affine_big(const ExtendParams& p, int grid, int threads, int mode, cudaStream_t st);
 
 }  // namespace phr

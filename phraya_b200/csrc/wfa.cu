@@ -1850,15 +1850,15 @@ void launch_wfa_linear_big(const ExtendParams& p, int grid, int mode, cudaStream
         wfa_linear_big_kernel<SeqB><<<grid, kBigThreads, p.big_smem, st>>>(p);
     }
 }
-void launch_wfa_affine_big(const ExtendParams& p, int grid, int mode, cudaStream_t st) {
+void launch_wfa_affine_big(const ExtendParams& p, int grid, int threads, int mode, cudaStream_t st) {
     if (mode == 0) {
         cudaFuncSetAttribute(wfa_affine_big_kernel<Seq2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(p.big_smem));
-        wfa_affine_big_kernel<Seq2><<<grid, kBigAffineThreads, p.big_smem, st>>>(p);
+        wfa_affine_big_kernel<Seq2><<<grid, threads, p.big_smem, st>>>(p);
     } else {
         cudaFuncSetAttribute(wfa_affine_big_kernel<SeqB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(p.big_smem));
-        wfa_affine_big_kernel<SeqB><<<grid, kBigAffineThreads, p.big_smem, st>>>(p);
+        wfa_affine_big_kernel<SeqB><<<grid, threads, p.big_smem, st>>>(p);
     }
 }
 

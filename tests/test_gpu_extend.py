@@ -220,6 +220,11 @@ def test_long_affine_pairs_cta_kernel(costs):
         e.set_timing(True)
         compare(e, A.ENGINE_WFA_AFFINE, pairs, costs)
         assert e.kernel_times().get("wfa_affine_big", (0, 0.0))[0] >= 1
+        # fewer threads per CTA (more CTAs per SM): the same results
+        for threads in (512, 256):
+            e.set_tune("wfa_affine_big_threads", threads)
+            compare(e, A.ENGINE_WFA_AFFINE, pairs, costs)
+        e.set_tune("wfa_affine_big_threads", 1024)
         # CTA kernel off: the warp-group kernel on the same pairs
         e.set_tune("wfa_big_min", 0)
         compare(e, A.ENGINE_WFA_AFFINE, pairs, costs)
@@ -232,6 +237,8 @@ def test_tune_keys_validated(eng):
         eng.set_tune("wfa_group_long", 3)
     with pytest.raises(P.EngineError):
         eng.set_tune("block_threads", 512)
+    with pytest.raises(P.EngineError):
+        eng.set_tune("wfa_affine_big_threads", 768)
     before = eng.get_tune("myers_band_base")
     eng.set_tune("myers_band_base", before)
     assert eng.get_tune("myers_band_base") == before
