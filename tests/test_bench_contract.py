@@ -80,3 +80,18 @@ def test_cpu_baseline_scales_sample(bench, sets):
     b = bench.cpu_baseline(set_a, set_b, 1_000_000, 1_000_000, 2, sample_a=500, sample_b=50)
     assert b["kind"] == "port" and b["cores"] == 2 and b["unit"] == "pairs/s" and b["value"] > 0
     assert "500 set-A pairs" in b["sample"]
+
+
+def test_read_parity_reports_first_mismatch(bench):
+    """Per-read parity counts mismatches over the checked reads and describes the first
+    one: outcome, has_result, reverse, then (ed, qs, qe, ts, te, CIGAR length) per
+    alignment, for the GPU and the oracle."""
+    row = (0, 1, 0, [("10M", 0, 0, 10, 5, 15)])
+    other = (4, 0, 0, [])
+    gpu = [row, other, row]
+    par = bench._read_parity(gpu, [row, row, row])
+    assert par["reads"] == 3 and par["mismatches"] == 1 and par["first_mismatch"] == 1
+    assert par["first_mismatch_detail"] == {"gpu": [4, 0, 0, []], "oracle": [0, 1, 0, [[0, 0, 10, 5, 15, 3]]]}
+    # a subset of the reads, by index
+    par = bench._read_parity(gpu, [row, row], [0, 2])
+    assert par == {"reads": 2, "mismatches": 0}
