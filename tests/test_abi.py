@@ -50,3 +50,17 @@ def test_status_strings():
     L = P.lib()
     for s in range(9):
         assert L.phr_status_string(s)
+
+
+def test_tune_keys_documented_in_header():
+    """Every launch-parameter key phr_ctx_set_tune accepts is documented in the header's
+    key list, and every documented key is accepted (read from the sources as text)."""
+    with open(os.path.join(ROOT, "phraya_b200", "csrc", "api.cu")) as f:
+        src = f.read()
+    body = src[src.index("int* tune_field("):src.index("bool tune_valid(")]
+    accepted = set(re.findall(r'strcmp\(key, "([a-z_0-9]+)"\)', body))
+    with open(os.path.join(ROOT, "include", "phraya_gpu.h")) as f:
+        hdr = f.read()
+    block = hdr[hdr.index("Launch parameters of the extension kernels"):hdr.index("phr_status phr_ctx_set_tune(")]
+    documented = set(re.findall(r'"([a-z_0-9]+)"', block))
+    assert accepted and accepted == documented, (accepted ^ documented)
