@@ -95,3 +95,33 @@ def test_read_parity_reports_first_mismatch(bench):
     # a subset of the reads, by index
     par = bench._read_parity(gpu, [row, row], [0, 2])
     assert par == {"reads": 2, "mismatches": 0}
+
+
+def test_reference_arm_keeps_the_job_mix(bench, monkeypatch):
+    """The reference arm's JSON line on small sizes, with the engine arm's generator run
+    on the CPU: the sample keeps the job's set-A : set-B proportion, and value,
+    ms_per_step and the projection agree."""
+    import contextlib
+    import io
+    import json
+    import types
+
+    from phraya_b200 import datagen as D
+
+    def arm_pairs_cpu(n_a, n_b, rank, dev):
+        return (D.extension_pairs_device(n_a, 100, 300, 0.05, seed=2 * rank, device="cpu"),
+                D.extension_pairs_device(n_b, 64, 2048, 0.05, seed=2 * rank + 1, log_uniform=True, device="cpu"))
+
+    monkeypatch.setattr(bench, "arm_pairs", arm_pairs_cpu)
+    monkeypatch.setattr(bench, "REF_SAMPLE_A", 200)
+    args = types.SimpleNamespace(n_a=2000, n_b=1000, steps=2, warmup=1, gpus=1)
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        bench.run_reference(args, 0, 1)
+    line = json.loads(buf.getvalue())
+    assert line["impl"] == "reference"
+    assert line["config"]["n_pairs_wfa"] == 200 and line["config"]["n_pairs_myers"] == 100
+    per_step = 2 * 200 + 100
+    assert line["value"] == pytest.approx(per_step / (line["ms_per_step"] / 1000.0))
+    assert line["projected_full_job_ms"] == pytest.approx((2 * 2000 + 1000) / line["value"] * 1000.0)
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
