@@ -496,6 +496,22 @@ def run_engine(args, rank, world):
             bad = [i for i in range(k) if g[i] != o[i]]
             micro_parity[nm] = {"pairs": k, "mismatches": len(bad), **({"first_mismatch": bad[0]} if bad else {})}
 
+    # every result of the timed job (all 3,000,000 alignments) through the size-independent
+    # checks (well-formed CIGAR, consumed spans, edit distance, whole query, global spans,
+    # affine score), outside the timed regions; no second implementation is needed
+    result_checks = None
+    if rank == 0:
+        from phraya_b200 import validate as V
+        from phraya_b200.batch import ALN_DTYPE
+        result_checks = {}
+        for (eng_id, costs, p, (aln, cig, _cap)), nm in zip(e2e_jobs, ("wfa_affine", "wfa_linear", "myers_global")):
+            try:
+                recs = np.frombuffer(aln.numpy(), dtype=ALN_DTYPE, count=p.n)
+                result_checks[nm] = V.check_extensions(eng_id, recs, cig.numpy(), p.q_len, costs, p.t_len)
+            except Exception as exc:  # a report, never a failed bench line
+                result_checks[nm] = {"error": f"{type(exc).__name__}: {exc}"}
+        log("microbench: size-independent checks of every result done")
+
     if rank != 0:
         return
     # ---- roofline of the dominant kernel (its device time per step, CUDA events) ----
@@ -564,6 +580,7 @@ def run_engine(args, rank, world):
             "clocks": clk,
             "cpu_baseline": cpu,
             "parity": micro_parity,
+            "result_checks": result_checks,
             "datagen_s": round(t_gen, 1),
             **cases}
     print(json.dumps(line))
