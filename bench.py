@@ -621,6 +621,16 @@ def _kernel_split(eng, fn):
             {k: eng.counter(k) for k in names})
 
 
+def _read_checks(res, packed, target_len):
+    """Size-independent checks of every alignment of an align_read call (res = rr, aln,
+    cigar, stats), as a report that never fails the bench line."""
+    try:
+        from phraya_b200 import validate as V
+        return V.check_read_alignments(res[0], res[1], res[2], packed.len, target_len)
+    except Exception as exc:
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def _read_parity(gpu, oracle_rows, idx=None):
     """Per-read comparison of unpacked GPU results (all reads) with oracle rows (the reads
     `idx`, or all): -> {"reads", "mismatches", "first_mismatch"}."""
@@ -778,6 +788,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
                        "wavefront_cells_per_s": work["wfa_linear_cells"] / med,
                        "roofline": _wfa_roofline(kms, work, int_peak, peak_src)}
     gpu_bal = P.unpack_reads(*res[:3])
+    out["balanced"]["result_checks"] = _read_checks(res, packed, len(ref))
     # sensitive (affine 2/4/1, 50 chains) on the first reads
     ns = min(args.long_sensitive, packed.n)
     sub = packed.subset(range(ns))
@@ -793,6 +804,7 @@ def run_long_reads(eng, dev, args, int_peak, peak_src):
                                "kernel_ms": dict(sorted(skms.items(), key=lambda kv: -kv[1])[:8]),
                                "roofline": _wfa_roofline(skms, swork, int_peak, peak_src)}
     gpu_sens = P.unpack_reads(*sres[:3])
+    out["sensitive_affine"]["result_checks"] = _read_checks(sres, sub, len(ref))
     out["clocks"] = clocks.stop()
     idx.close()
     if not args.no_cpu:
@@ -871,6 +883,7 @@ def run_contigs_protein(eng, dev, args):
                            "scratch_oom_pairs": eng.counter("scratch_oom_pairs"),
                            "kernel_ms": dict(sorted(kms.items(), key=lambda kv: -kv[1])[:8])})
     gpu_c = P.unpack_reads(*res[:3])
+    out["contigs"]["result_checks"] = _read_checks(res, packed, len(ref))
     # protein pairs through the four engines (host buffers), and protein align_read
     pairs = G.protein_pairs(5000, seed=402)
     pp = PackedPairs(pairs)

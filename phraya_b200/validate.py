@@ -121,3 +121,23 @@ def check_extensions(engine, aln, cigar, q_len, costs=None, t_len=None):
         out["affine_score"] = int((cost != a["affine_score"].astype(np.int64)).sum())
     out["violations"] = int(sum(v for k, v in out.items() if k != "checked"))
     return out
+
+
+def check_read_alignments(rr, aln, cigar, read_len, target_len):
+    """The same checks for align_read results (rr: READ_RESULT_DTYPE per read, whose
+    alignments are aln[aln_off .. aln_off + n_aln)): every alignment of a read spans the
+    whole read (query_start 0, query_end its length, in the orientation it was aligned
+    in) and ends inside the target; plus well-formed CIGARs, consumed spans and edit
+    distance = X + I + D. The alignments mix engines, so the affine score is not checked."""
+    n_aln = np.asarray(rr["n_aln"], dtype=np.int64)
+    first = np.asarray(rr["aln_off"], dtype=np.int64)
+    owner = np.repeat(np.arange(len(rr), dtype=np.int64), n_aln)
+    within = np.arange(owner.size, dtype=np.int64) - np.repeat(np.cumsum(n_aln) - n_aln, n_aln)
+    idx = np.repeat(first, n_aln) + within
+    sub = aln[idx]
+    out = check_extensions(-1, sub, cigar, np.asarray(read_len, dtype=np.int64)[owner])
+    ok = sub["status"] == A.PHR_OK
+    out["query_start_not_zero"] = int(((sub["query_start"] != 0) & ok).sum())
+    out["target_beyond_end"] = int(((sub["target_end"].astype(np.int64) > int(target_len)) & ok).sum())
+    out["violations"] = int(sum(v for k, v in out.items() if k not in ("checked", "violations")))
+    return out

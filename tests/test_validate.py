@@ -76,3 +76,27 @@ def test_planted_mistakes_are_counted(sets):
     a = aln.copy()
     a["status"][:10] = A.PHR_ALIGNMENT_FAILED
     assert check(a, cig)["checked"] == aln.size - 10
+
+
+def test_read_alignments_pass_and_plants_are_counted():
+    """align_read results of the oracle (short and long reads, every strategy) pass the
+    read-level checks; a planted start, end or distance mistake is counted."""
+    ref = D.random_reference(200_000, seed=5)
+    reads, _, _ = D.reads_on_reference(ref, 400, 150, 0.02, seed=6)
+    lreads, _, _ = D.reads_on_reference(
+        ref, 20, error=0.05, seed=8, sub_frac=0.4, max_indel=3,
+        length_sampler=lambda g, n: np.clip(np.exp(g.normal(np.log(3000), 0.5, n)), 1000, 8000).astype(np.int64))
+    otg = O.Target(ref)
+    for rd in (reads, lreads):
+        for strat in (A.BALANCED, A.SENSITIVE, A.FAST):
+            rr, aln, cig, _ = otg.align_packed(rd, strat, A.GAP_AFFINE)
+            r = V.check_read_alignments(rr, aln, cig, rd.len, len(ref))
+            assert r["checked"] > 0 and r["violations"] == 0, r
+    rr, aln, cig, _ = otg.align_packed(reads, A.BALANCED, A.GAP_AFFINE)
+    a = aln.copy()
+    a["query_start"][0] += 1
+    a["target_end"][1] = len(ref) + 5
+    a["edit_distance"][2] += 1
+    r = V.check_read_alignments(rr, a, cig, reads.len, len(ref))
+    assert r["query_start_not_zero"] == 1 and r["target_beyond_end"] == 1 and r["edit_distance"] == 1
+    assert r["violations"] >= 3
