@@ -33,31 +33,32 @@ def parse_runs(aln, cigar, idx):
     off = aln["cigar_off"][idx].astype(np.int64)
     ln = aln["cigar_len"][idx].astype(np.int64)
     n = len(idx)
-    bad = np.zeros(n, dtype=bool)
+    bad = ln == 0
     total = int(ln.sum())
     if total == 0:
         e = np.zeros(0, dtype=np.int64)
-        return e, e, e, bad | (ln == 0)
-    # the bytes of the checked texts, concatenated, with their owner
-    owner_b = np.repeat(np.arange(n, dtype=np.int64), ln)
-    starts = np.cumsum(ln) - ln
-    pos = np.arange(total, dtype=np.int64) - np.repeat(starts, ln) + np.repeat(off, ln)
-    if pos.size and (pos.max() >= cig.size):
-        raise ValueError("a CIGAR reaches past the text arena")
-    b = cig[pos]
+        return e, e, e, bad
+    starts = np.cumsum(ln) - ln  # of each text in the concatenation
+    if (off[0] + total <= cig.size) and (n == 1 or np.array_equal(off[1:], off[:-1] + ln[:-1])):
+        b = cig[off[0]:off[0] + total]  # the texts lie back to back in the arena: a view
+    else:
+        pos = np.arange(total, dtype=np.int64) - np.repeat(starts, ln) + np.repeat(off, ln)
+        if pos.max() >= cig.size:
+            raise ValueError("a CIGAR reaches past the text arena")
+        b = cig[pos]
     is_digit = (b >= ord("0")) & (b <= ord("9"))
-    op_code = np.full(b.shape, -1, dtype=np.int64)
+    op_code = np.full(b.shape, -1, dtype=np.int8)
     for c, ch in enumerate(_OPS):
         op_code[b == ch] = c
     is_op = op_code >= 0
     # every byte is a digit or an op, and every text ends with an op
-    np.logical_or.at(bad, owner_b, ~(is_digit | is_op))
-    last = starts + ln - 1
-    bad |= (ln == 0)
-    ok_last = ln > 0
-    bad[ok_last] |= ~is_op[last[ok_last]]
+    stray = np.flatnonzero(~(is_digit | is_op))
+    if stray.size:
+        bad[np.searchsorted(starts, stray, side="right") - 1] = True
+    nz = ~bad
+    bad[nz] |= ~is_op[(starts + ln - 1)[nz]]
     op_at = np.flatnonzero(is_op)
-    owner = owner_b[op_at]
+    owner = np.searchsorted(starts, op_at, side="right") - 1
     # digits of each run: the bytes between the previous op of the same text (or the text's
     # start) and this op
     prev_end = np.empty_like(op_at)
@@ -67,22 +68,22 @@ def parse_runs(aln, cigar, idx):
     first_of_text[1:] = owner[1:] != owner[:-1]
     prev_end[first_of_text] = starts[owner[first_of_text]]
     ndig = op_at - prev_end
-    np.logical_or.at(bad, owner, (ndig < 1) | (ndig > 9))
     count = np.zeros(op_at.size, dtype=np.int64)
-    digit = np.where(is_digit, b.astype(np.int64) - ord("0"), 0)
     scale = np.ones(op_at.size, dtype=np.int64)
     for d in range(1, 10):
-        use = ndig >= d
-        if not use.any():
+        use = np.flatnonzero(ndig >= d)
+        if use.size == 0:
             break
-        count[use] += digit[op_at[use] - d] * scale[use]
+        count[use] += (b[op_at[use] - d].astype(np.int64) - ord("0")) * scale[use]
         scale[use] *= 10
-    # counts are >= 1 and written without leading zeros
+    # counts are >= 1 and written without leading zeros, with 1 to 9 digits
     has = ndig >= 1
     lead_zero = np.zeros(op_at.size, dtype=bool)
     lead_zero[has] = b[prev_end[has]] == ord("0")
-    np.logical_or.at(bad, owner, (count < 1) | lead_zero)
-    return owner, count, op_code[op_at], bad
+    wrong = (ndig < 1) | (ndig > 9) | (count < 1) | lead_zero
+    if wrong.any():
+        bad[owner[wrong]] = True
+    return owner, count, op_code[op_at].astype(np.int64), bad
 
 
 def check_extensions(engine, aln, cigar, q_len, costs=None, t_len=None):
