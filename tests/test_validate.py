@@ -100,3 +100,17 @@ def test_read_alignments_pass_and_plants_are_counted():
     r = V.check_read_alignments(rr, a, cig, reads.len, len(ref))
     assert r["query_start_not_zero"] == 1 and r["target_beyond_end"] == 1 and r["edit_distance"] == 1
     assert r["violations"] >= 3
+
+
+def test_texts_not_back_to_back(sets):
+    """Checking a subset whose texts are not adjacent in the arena (every other pair
+    failed) reads them one by one and finds the same (clean) results, and still catches a
+    planted mistake."""
+    pk = sets[0]
+    aln, cig = O.extend_packed(A.ENGINE_WFA_LINEAR, pk, (2, 4, 1))
+    a = aln.copy()
+    a["status"][::2] = A.PHR_ALIGNMENT_FAILED
+    r = V.check_extensions(A.ENGINE_WFA_LINEAR, a, cig, pk.q_len)
+    assert r["checked"] == aln.size // 2 and r["violations"] == 0, r
+    a["edit_distance"][1] += 3
+    assert V.check_extensions(A.ENGINE_WFA_LINEAR, a, cig, pk.q_len)["edit_distance"] == 1
