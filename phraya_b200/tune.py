@@ -2,7 +2,8 @@
 
 The kernels' results never depend on these settings (lanes per WFA pair, the length
 bucket edge between short and long WFA pairs, threads per block, resident blocks per
-SM, the Myers stored-band base, the threshold of the one-CTA-per-pair WFA kernel);
+SM, the Myers stored-band base and checkpointing, the threshold of the one-CTA-per-pair
+WFA kernels and the gap-affine one's threads per CTA);
 only their speed does. The tuner runs a coordinate descent over a small candidate grid
 per key: for each key in turn it times every candidate on the given workloads with the
 other keys at their current best, keeps the fastest, and repeats the sweep. Time is the
@@ -29,17 +30,19 @@ SPACE = {
     "wfa_long_min": [512, 1024, 2048],
     "block_threads": [128, 256],
     "max_blocks_per_sm": [2, 3, 4],
-    "myers_band_base": [32, 64, 128],
+    "myers_band_base": [32, 48, 64, 128],
+    "myers_lane_ckpt": [0, 1],
     "wfa_big_min": [0, 2048, 4096, 8192],
+    "wfa_affine_big_threads": [256, 512, 1024],
 }
 
 KEYS_FOR = {
     A.ENGINE_WFA_LINEAR: ["wfa_group_short", "wfa_group_long", "wfa_long_min", "block_threads",
                           "max_blocks_per_sm", "wfa_big_min"],
     A.ENGINE_WFA_AFFINE: ["wfa_affine_group_short", "wfa_group_long", "wfa_long_min", "block_threads",
-                          "max_blocks_per_sm"],
+                          "max_blocks_per_sm", "wfa_big_min", "wfa_affine_big_threads"],
     A.ENGINE_MYERS_FIT: ["myers_band_base", "block_threads", "max_blocks_per_sm"],
-    A.ENGINE_MYERS_GLOBAL: ["myers_band_base", "block_threads", "max_blocks_per_sm"],
+    A.ENGINE_MYERS_GLOBAL: ["myers_band_base", "myers_lane_ckpt", "block_threads", "max_blocks_per_sm"],
 }
 
 

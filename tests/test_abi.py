@@ -64,3 +64,16 @@ def test_tune_keys_documented_in_header():
     block = hdr[hdr.index("Launch parameters of the extension kernels"):hdr.index("phr_status phr_ctx_set_tune(")]
     documented = set(re.findall(r'"([a-z_0-9]+)"', block))
     assert accepted and accepted == documented, (accepted ^ documented)
+
+
+def test_autotuner_keys_are_library_keys():
+    """Every key the autotuner searches, and every key it assigns to an engine, is one the
+    library accepts (documented in the header's key list)."""
+    from phraya_b200 import tune as T
+    with open(os.path.join(ROOT, "include", "phraya_gpu.h")) as f:
+        hdr = f.read()
+    block = hdr[hdr.index("Launch parameters of the extension kernels"):hdr.index("phr_status phr_ctx_set_tune(")]
+    documented = set(re.findall(r'"([a-z_0-9]+)"', block))
+    assert set(T.SPACE) <= documented
+    for keys in T.KEYS_FOR.values():
+        assert set(keys) <= set(T.SPACE)
